@@ -1,0 +1,684 @@
+// C ABI of libefm.so (declared in include/efm.h): instance bookkeeping, workspace, and the
+// time loops that replace the reference's Python per-step loops
+// (Elastic3D.forwardFields :1812-1847, backwardFields_FowardFieldsRemake :1929-2054,
+// backwardFields :2056-2082).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "efm.h"
+#include "efm_internal.cuh"
+#include "efm_util.cuh"
+
+extern "C" cudaError_t efm_launch_stress(int pass, const EfmInst *insts, int ninst, int tiles,
+                                         int it, cudaStream_t s);
+extern "C" cudaError_t efm_launch_velocity(int pass, const EfmInst *insts, int ninst, int tiles,
+                                           int it, cudaStream_t s);
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define EFM_CK(call)                                                                        \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(EFM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct Inst {
+    int nx = 0, ny = 0, nz = 0, W = 0, nt = 0, nsrc = 0, nrec = 0;
+    float dx = 0.f, dt = 0.f;
+    const float *lam = nullptr, *mu = nullptr, *rho = nullptr, *wav = nullptr;
+    int src[EFM_NSRC][3] = {};
+    float mt[EFM_NSRC][6] = {};
+    std::vector<float> cpml_host;
+    std::vector<int> rec;  // [nrec][3]
+    // device data owned by the library
+    float *cpml = nullptr;
+    uint32_t *rec_mask = nullptr;
+    int *rec_lin = nullptr, *rec_id = nullptr;
+    float *fields = nullptr;  // va(3) t(6) | vb(3) bv(3) bt(6) when gradient-capable
+    bool fields_grad = false;
+    float *psi = nullptr;
+    float *border = nullptr;
+    int64_t ncell = 0, strip_n = 0, psx_n = 0, psy_n = 0, psz_n = 0;
+    int64_t gather_off = 0, grad_off = 0;
+    int tiles_x = 0, tiles_z = 0, tiles_y = 0, tiles = 0, tile_begin = 0;
+    bool fwd_saved = false;
+
+    float *va(int c) const { return fields + c * ncell; }
+    float *tt(int c) const { return fields + (3 + c) * ncell; }
+    float *vb(int c) const { return fields + (9 + c) * ncell; }
+    float *bv(int c) const { return fields + (12 + c) * ncell; }
+    float *bt(int c) const { return fields + (15 + c) * ncell; }
+};
+
+// per-device scratch of the deterministic reductions
+struct Scratch {
+    double *partial = nullptr;
+    int64_t *seg = nullptr;
+    size_t cap = 0, seg_cap = 0;
+};
+std::mutex g_scratch_mu;
+Scratch g_scratch[64];
+
+int get_scratch(int nseg, double **partial, int64_t **seg) {
+    int dev = 0;
+    EFM_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(EFM_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    Scratch &S = g_scratch[dev];
+    const size_t need = (size_t)nseg * EFM_RED_BLOCKS;
+    if (S.cap < need) {
+        if (S.partial) cudaFree(S.partial);
+        S.partial = nullptr;
+        S.cap = 0;
+        EFM_CK(cudaMalloc(&S.partial, need * sizeof(double)));
+        S.cap = need;
+    }
+    if (S.seg_cap < (size_t)nseg + 1) {
+        if (S.seg) cudaFree(S.seg);
+        S.seg = nullptr;
+        S.seg_cap = 0;
+        EFM_CK(cudaMalloc(&S.seg, ((size_t)nseg + 1) * sizeof(int64_t)));
+        S.seg_cap = nseg + 1;
+    }
+    *partial = S.partial;
+    *seg = S.seg;
+    return EFM_OK;
+}
+
+}  // namespace
+
+struct efm_ctx {
+    std::vector<Inst> inst;
+    EfmInst *d_tab = nullptr;  // 4 tables: FWD, ADJ, REV parity 0, REV parity 1
+    int tab_cap = 0;
+    int total_tiles = 0;
+    int64_t gather_total = 0;
+    std::vector<int64_t> seg_host;
+    int64_t *d_seg = nullptr;  // gather-layout segment offsets (ninst + 1)
+    double *d_partial = nullptr;
+    bool layout_ready = false;
+    // measurement
+    int64_t launches[EFM_NKERN] = {};
+    double ms[EFM_NKERN] = {};
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;       // created on demand, reused
+    std::vector<std::pair<int, int>> ev_used;  // (kind, first event index) of pending pairs
+};
+
+namespace {
+
+// Launch through this wrapper so every kernel is counted (and timed when enabled).
+template <class F>
+int timed_launch(efm_ctx *ctx, int kind, cudaStream_t s, F &&launch) {
+    ctx->launches[kind] += 1;
+    int i0 = -1;
+    if (ctx->timing) {
+        i0 = (int)ctx->ev_used.size() * 2;
+        while ((int)ctx->ev_pool.size() < i0 + 2) {
+            cudaEvent_t e;
+            EFM_CK(cudaEventCreate(&e));
+            ctx->ev_pool.push_back(e);
+        }
+        EFM_CK(cudaEventRecord(ctx->ev_pool[i0], s));
+    }
+    EFM_CK(launch());
+    if (ctx->timing) {
+        EFM_CK(cudaEventRecord(ctx->ev_pool[i0 + 1], s));
+        ctx->ev_used.push_back({kind, i0});
+    }
+    return EFM_OK;
+}
+
+int collect_times(efm_ctx *ctx) {
+    for (auto &p : ctx->ev_used) {
+        EFM_CK(cudaEventSynchronize(ctx->ev_pool[p.second + 1]));
+        float ms = 0.f;
+        EFM_CK(cudaEventElapsedTime(&ms, ctx->ev_pool[p.second], ctx->ev_pool[p.second + 1]));
+        ctx->ms[p.first] += ms;
+    }
+    ctx->ev_used.clear();
+    return EFM_OK;
+}
+
+int64_t strip_count(const Inst &I) {
+    const int64_t bx = I.nx - 2 * I.W, by = I.ny - 2 * I.W, bz = I.nz - I.W - 2;
+    return 4 * by * bz + 4 * bz * bx + 4 * by * bx;
+}
+
+void free_inst(Inst &I) {
+    cudaFree(I.cpml);
+    cudaFree(I.rec_mask);
+    cudaFree(I.rec_lin);
+    cudaFree(I.rec_id);
+    cudaFree(I.fields);
+    cudaFree(I.psi);
+    cudaFree(I.border);
+    I.cpml = nullptr;
+    I.rec_mask = nullptr;
+    I.rec_lin = I.rec_id = nullptr;
+    I.fields = I.psi = I.border = nullptr;
+}
+
+// tile offsets, gather offsets and the small device tables
+int ensure_layout(efm_ctx *ctx) {
+    if (ctx->layout_ready) return EFM_OK;
+    const int n = (int)ctx->inst.size();
+    int tiles = 0;
+    int64_t goff = 0, gr = 0;
+    ctx->seg_host.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        Inst &I = ctx->inst[i];
+        I.tile_begin = tiles;
+        tiles += I.tiles;
+        I.gather_off = goff;
+        ctx->seg_host[i] = goff;
+        goff += 3LL * I.nt * I.nrec;
+        I.grad_off = gr;
+        gr += 3 * I.ncell;
+    }
+    ctx->seg_host[n] = goff;
+    ctx->total_tiles = tiles;
+    ctx->gather_total = goff;
+    if (ctx->tab_cap < n) {
+        cudaFree(ctx->d_tab);
+        ctx->d_tab = nullptr;
+        cudaFree(ctx->d_seg);
+        ctx->d_seg = nullptr;
+        cudaFree(ctx->d_partial);
+        ctx->d_partial = nullptr;
+        ctx->tab_cap = 0;
+        EFM_CK(cudaMalloc(&ctx->d_tab, 4 * (size_t)n * sizeof(EfmInst)));
+        EFM_CK(cudaMalloc(&ctx->d_seg, ((size_t)n + 1) * sizeof(int64_t)));
+        EFM_CK(cudaMalloc(&ctx->d_partial, (size_t)n * EFM_RED_BLOCKS * sizeof(double)));
+        ctx->tab_cap = n;
+    }
+    EFM_CK(cudaMemcpy(ctx->d_seg, ctx->seg_host.data(), (n + 1) * sizeof(int64_t),
+                      cudaMemcpyHostToDevice));
+    ctx->layout_ready = true;
+    return EFM_OK;
+}
+
+int ensure_workspace(efm_ctx *ctx, bool grad, bool borders) {
+    for (Inst &I : ctx->inst) {
+        const int nfields = grad ? 21 : 9;
+        if (I.fields == nullptr || (grad && !I.fields_grad)) {
+            float *nf = nullptr;
+            if (cudaMalloc(&nf, (size_t)nfields * I.ncell * sizeof(float)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(EFM_ERR_NOMEM, "cannot allocate wavefields (" +
+                                               std::to_string((size_t)nfields * I.ncell * 4) +
+                                               " bytes)");
+            }
+            cudaFree(I.fields);
+            I.fields = nf;
+            I.fields_grad = grad;
+            I.fwd_saved = false;
+        }
+        if (I.psi == nullptr) {
+            const size_t np = 6 * (size_t)(I.psx_n + I.psy_n + I.psz_n);
+            if (cudaMalloc(&I.psi, np * sizeof(float)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(EFM_ERR_NOMEM, "cannot allocate CPML memory variables");
+            }
+        }
+        if (borders && I.border == nullptr) {
+            const size_t nb = (size_t)I.nt * 3 * I.strip_n;
+            if (cudaMalloc(&I.border, nb * sizeof(float)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(EFM_ERR_NOMEM, "cannot allocate boundary strips (" +
+                                               std::to_string(nb * 4) + " bytes)");
+            }
+        }
+    }
+    return EFM_OK;
+}
+
+EfmInst base_table(const Inst &I) {
+    EfmInst d;
+    std::memset(&d, 0, sizeof(d));
+    d.nx = I.nx;
+    d.ny = I.ny;
+    d.nz = I.nz;
+    d.W = I.W;
+    d.tiles_x = I.tiles_x;
+    d.tiles_z = I.tiles_z;
+    d.tiles_y = I.tiles_y;
+    d.tile_begin = I.tile_begin;
+    d.nt = I.nt;
+    d.k = I.dt / I.dx;  // float32 quotient, as the reference's (dt/dx)
+    d.inv_dt = 1.0f / I.dt;
+    d.inv_dx = 1.0f / I.dx;
+    d.lam = I.lam;
+    d.mu = I.mu;
+    d.rho = I.rho;
+    d.cpml = I.cpml;
+    d.psi_x = I.psi;
+    d.psi_y = I.psi + 6 * I.psx_n;
+    d.psi_z = I.psi + 6 * (I.psx_n + I.psy_n);
+    d.nsrc = I.nsrc;
+    for (int s = 0; s < EFM_NSRC; ++s) {
+        d.sx[s] = I.src[s][0];
+        d.sy[s] = I.src[s][1];
+        d.sz[s] = I.src[s][2];
+        for (int c = 0; c < 6; ++c) d.mt[s][c] = I.mt[s][c];
+    }
+    d.wav = I.wav;
+    d.nrec = I.nrec;
+    d.rec_mask = I.rec_mask;
+    d.rec_lin = I.rec_lin;
+    d.rec_id = I.rec_id;
+    d.strip_n = I.strip_n;
+    return d;
+}
+
+int zero_psi(const Inst &I, cudaStream_t s) {
+    EFM_CK(cudaMemsetAsync(I.psi, 0, 6 * (size_t)(I.psx_n + I.psy_n + I.psz_n) * sizeof(float), s));
+    return EFM_OK;
+}
+
+int check_ready(efm_ctx *ctx) {
+    if (ctx == nullptr) return fail(EFM_ERR_ARG, "null context");
+    if (ctx->inst.empty()) return fail(EFM_ERR_STATE, "no instances");
+    for (size_t i = 0; i < ctx->inst.size(); ++i) {
+        const Inst &I = ctx->inst[i];
+        if (!I.lam || !I.mu || !I.rho || !I.wav)
+            return fail(EFM_ERR_STATE, "instance " + std::to_string(i) + " has no model/wavelet");
+    }
+    return ensure_layout(ctx);
+}
+
+}  // namespace
+
+// ============================================================================ C ABI
+extern "C" {
+
+const char *efm_last_error(void) { return g_err.c_str(); }
+int efm_version(void) { return 1; }
+
+int efm_create(efm_ctx **out) {
+    if (out == nullptr) return fail(EFM_ERR_ARG, "null out pointer");
+    *out = new efm_ctx();
+    return EFM_OK;
+}
+
+int efm_clear(efm_ctx *ctx) {
+    if (ctx == nullptr) return fail(EFM_ERR_ARG, "null context");
+    for (Inst &I : ctx->inst) free_inst(I);
+    ctx->inst.clear();
+    ctx->layout_ready = false;
+    return EFM_OK;
+}
+
+int efm_destroy(efm_ctx *ctx) {
+    if (ctx == nullptr) return EFM_OK;
+    efm_clear(ctx);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    cudaFree(ctx->d_tab);
+    cudaFree(ctx->d_seg);
+    cudaFree(ctx->d_partial);
+    delete ctx;
+    return EFM_OK;
+}
+
+int efm_num_instances(const efm_ctx *ctx) { return ctx ? (int)ctx->inst.size() : 0; }
+
+int efm_add_instance(efm_ctx *ctx, const efm_instance_desc *d, int *id) {
+    if (ctx == nullptr || d == nullptr) return fail(EFM_ERR_ARG, "null argument");
+    const int W = d->lenpml;
+    if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0) return fail(EFM_ERR_ARG, "grid dims must be > 0");
+    if (W < EFM_HS) return fail(EFM_ERR_ARG, "lenpml must be >= 2");
+    if (d->nx - 2 * W < 4 || d->ny - 2 * W < 4 || d->nz - W - 2 < 4)
+        return fail(EFM_ERR_ARG, "grid too small for the CPML width (need nx,ny >= 2W+4, nz >= W+6)");
+    if ((int64_t)d->nx * d->ny * d->nz >= (1LL << 31))
+        return fail(EFM_ERR_ARG, "grid has 2^31 cells or more");
+    if (!(d->dx > 0.f) || !(d->dt > 0.f)) return fail(EFM_ERR_ARG, "dx and dt must be > 0");
+    if (d->nt < 2) return fail(EFM_ERR_ARG, "nt must be >= 2");
+    if (d->nsrc < 1 || d->nsrc > EFM_NSRC) return fail(EFM_ERR_ARG, "nsrc must be in 1..4");
+    if (d->nrec < 1) return fail(EFM_ERR_ARG, "nrec must be >= 1");
+    if (!d->cpml_host || !d->src_host || !d->mt_host || !d->rec_host)
+        return fail(EFM_ERR_ARG, "null host array");
+    Inst I;
+    I.nx = d->nx;
+    I.ny = d->ny;
+    I.nz = d->nz;
+    I.W = W;
+    I.nt = d->nt;
+    I.dx = d->dx;
+    I.dt = d->dt;
+    I.nsrc = d->nsrc;
+    I.nrec = d->nrec;
+    I.lam = d->lam_dev;
+    I.mu = d->mu_dev;
+    I.rho = d->rho_dev;
+    I.wav = d->wavelet_dev;
+    for (int s = 0; s < d->nsrc; ++s) {
+        for (int c = 0; c < 3; ++c) I.src[s][c] = d->src_host[3 * s + c];
+        for (int c = 0; c < 6; ++c) I.mt[s][c] = d->mt_host[6 * s + c];
+        const int sx = I.src[s][0], sy = I.src[s][1], sz = I.src[s][2];
+        if (sx < EFM_HS || sx >= I.nx - EFM_HS || sy < EFM_HS || sy >= I.ny - EFM_HS || sz < EFM_HS ||
+            sz >= I.nz - EFM_HS)
+            return fail(EFM_ERR_ARG, "source outside the updated interior [2, n-2)");
+    }
+    I.rec.assign(d->rec_host, d->rec_host + 3 * d->nrec);
+    for (int r = 0; r < d->nrec; ++r) {
+        const int x = I.rec[3 * r], y = I.rec[3 * r + 1], z = I.rec[3 * r + 2];
+        if (x < 0 || x >= I.nx || y < 0 || y >= I.ny || z < 0 || z >= I.nz)
+            return fail(EFM_ERR_ARG, "receiver outside the grid");
+    }
+    const int nc = 2 * (I.nx + I.ny + I.nz);
+    I.cpml_host.assign(d->cpml_host, d->cpml_host + nc);
+    I.ncell = (int64_t)I.nx * I.ny * I.nz;
+    I.strip_n = strip_count(I);
+    I.psx_n = (int64_t)I.ny * I.nz * 2 * W;
+    I.psy_n = (int64_t)2 * W * I.nz * I.nx;
+    I.psz_n = (int64_t)I.ny * W * I.nx;
+    I.tiles_x = (I.nx + EFM_TX - 1) / EFM_TX;
+    I.tiles_z = (I.nz + EFM_TZ - 1) / EFM_TZ;
+    I.tiles_y = (I.ny + EFM_TY - 1) / EFM_TY;
+    I.tiles = I.tiles_x * I.tiles_z * I.tiles_y;
+
+    // receivers: bit mask + sorted (cell, receiver) list
+    const int nw = (I.nx + 31) / 32;
+    std::vector<uint32_t> mask((size_t)I.ny * I.nz * nw, 0u);
+    std::vector<std::pair<int, int>> lr(I.nrec);
+    for (int r = 0; r < I.nrec; ++r) {
+        const int x = I.rec[3 * r], y = I.rec[3 * r + 1], z = I.rec[3 * r + 2];
+        mask[((size_t)y * I.nz + z) * nw + (x >> 5)] |= 1u << (x & 31);
+        lr[r] = {x + I.nx * (z + I.nz * y), r};
+    }
+    std::sort(lr.begin(), lr.end());
+    std::vector<int> lin(I.nrec), rid(I.nrec);
+    for (int r = 0; r < I.nrec; ++r) {
+        lin[r] = lr[r].first;
+        rid[r] = lr[r].second;
+    }
+    auto bad = [&](cudaError_t e) {
+        free_inst(I);
+        return fail(EFM_ERR_CUDA, std::string("instance upload: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&I.cpml, nc * sizeof(float)))) return bad(e);
+    if ((e = cudaMalloc(&I.rec_mask, mask.size() * sizeof(uint32_t)))) return bad(e);
+    if ((e = cudaMalloc(&I.rec_lin, I.nrec * sizeof(int)))) return bad(e);
+    if ((e = cudaMalloc(&I.rec_id, I.nrec * sizeof(int)))) return bad(e);
+    if ((e = cudaMemcpy(I.cpml, I.cpml_host.data(), nc * sizeof(float), cudaMemcpyHostToDevice))) return bad(e);
+    if ((e = cudaMemcpy(I.rec_mask, mask.data(), mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice))) return bad(e);
+    if ((e = cudaMemcpy(I.rec_lin, lin.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
+    if ((e = cudaMemcpy(I.rec_id, rid.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
+    ctx->inst.push_back(std::move(I));
+    ctx->layout_ready = false;
+    if (id) *id = (int)ctx->inst.size() - 1;
+    return EFM_OK;
+}
+
+int efm_set_model(efm_ctx *ctx, int id, const float *lam, const float *mu, const float *rho) {
+    if (ctx == nullptr || id < 0 || id >= (int)ctx->inst.size())
+        return fail(EFM_ERR_ARG, "bad instance id");
+    if (!lam || !mu || !rho) return fail(EFM_ERR_ARG, "null model pointer");
+    Inst &I = ctx->inst[id];
+    I.lam = lam;
+    I.mu = mu;
+    I.rho = rho;
+    return EFM_OK;
+}
+
+int efm_set_moment_tensor(efm_ctx *ctx, int id, const float *mt) {
+    if (ctx == nullptr || id < 0 || id >= (int)ctx->inst.size())
+        return fail(EFM_ERR_ARG, "bad instance id");
+    if (!mt) return fail(EFM_ERR_ARG, "null moment tensor");
+    Inst &I = ctx->inst[id];
+    for (int s = 0; s < I.nsrc; ++s)
+        for (int c = 0; c < 6; ++c) I.mt[s][c] = mt[6 * s + c];
+    return EFM_OK;
+}
+
+int64_t efm_gather_size(const efm_ctx *ctx) {
+    if (!ctx) return -1;
+    int64_t n = 0;
+    for (const Inst &I : ctx->inst) n += 3LL * I.nt * I.nrec;
+    return n;
+}
+
+int64_t efm_gather_offset(const efm_ctx *ctx, int id) {
+    if (!ctx || id < 0 || id >= (int)ctx->inst.size()) return -1;
+    int64_t n = 0;
+    for (int i = 0; i < id; ++i) n += 3LL * ctx->inst[i].nt * ctx->inst[i].nrec;
+    return n;
+}
+
+int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders) {
+    if (!ctx) return -1;
+    int64_t b = 0;
+    for (const Inst &I : ctx->inst) {
+        b += (save_borders ? 21 : 9) * I.ncell * 4;
+        b += 6 * (I.psx_n + I.psy_n + I.psz_n) * 4;
+        if (save_borders) b += (int64_t)I.nt * 3 * I.strip_n * 4;
+    }
+    return b;
+}
+
+int efm_forward(efm_ctx *ctx, float *gathers, int save_borders, void *stream) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (gathers == nullptr) return fail(EFM_ERR_ARG, "null gathers");
+    cudaStream_t s = (cudaStream_t)stream;
+    if ((rc = ensure_workspace(ctx, save_borders != 0, save_borders != 0))) return rc;
+    const int n = (int)ctx->inst.size();
+    std::vector<EfmInst> tab(n);
+    int maxnt = 0;
+    for (int i = 0; i < n; ++i) {
+        Inst &I = ctx->inst[i];
+        EFM_CK(cudaMemsetAsync(I.fields, 0, 9 * I.ncell * sizeof(float), s));
+        if ((rc = zero_psi(I, s))) return rc;
+        EfmInst d = base_table(I);
+        d.nsteps = I.nt;
+        for (int c = 0; c < 3; ++c) d.f.v[c] = d.f.vo[c] = I.va(c);
+        for (int c = 0; c < 6; ++c) d.f.t[c] = I.tt(c);
+        d.gather = gathers + I.gather_off;
+        d.border = save_borders ? I.border : nullptr;
+        tab[i] = d;
+        maxnt = std::max(maxnt, I.nt);
+        I.fwd_saved = false;
+    }
+    EFM_CK(cudaMemcpyAsync(ctx->d_tab, tab.data(), n * sizeof(EfmInst), cudaMemcpyHostToDevice, s));
+    for (int it = 0; it < maxnt; ++it) {
+        if ((rc = timed_launch(ctx, EFM_K_FWD_STRESS, s, [&] {
+                 return efm_launch_stress(EFM_FWD, ctx->d_tab, n, ctx->total_tiles, it, s);
+             })))
+            return rc;
+        if ((rc = timed_launch(ctx, EFM_K_FWD_VELOCITY, s, [&] {
+                 return efm_launch_velocity(EFM_FWD, ctx->d_tab, n, ctx->total_tiles, it, s);
+             })))
+            return rc;
+    }
+    for (Inst &I : ctx->inst) I.fwd_saved = save_borders != 0;
+    return EFM_OK;
+}
+
+int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int flags,
+                 void *stream) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    const bool model = (flags & EFM_GRAD_MODEL) != 0, mt = (flags & EFM_GRAD_MT) != 0;
+    if (!model && !mt) return fail(EFM_ERR_ARG, "flags select no gradient");
+    if (res == nullptr) return fail(EFM_ERR_ARG, "null residual");
+    if (model && grad == nullptr) return fail(EFM_ERR_ARG, "null gradient buffer");
+    if (mt && mtg == nullptr) return fail(EFM_ERR_ARG, "null MT gradient buffer");
+    if ((rc = ensure_workspace(ctx, true, false))) return rc;
+    if (model)
+        for (const Inst &I : ctx->inst)
+            if (!I.fwd_saved)
+                return fail(EFM_ERR_STATE,
+                            "EFM_GRAD_MODEL needs a preceding efm_forward(..., save_borders=1)");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = (int)ctx->inst.size();
+    std::vector<EfmInst> tab(4 * (size_t)n);
+    int maxsteps = 0;
+    for (int i = 0; i < n; ++i) {
+        Inst &I = ctx->inst[i];
+        EFM_CK(cudaMemsetAsync(I.bv(0), 0, 9 * I.ncell * sizeof(float), s));  // bv, bt
+        if ((rc = zero_psi(I, s))) return rc;  // adjoint CPML memory (forward's is unused now)
+        if (model) EFM_CK(cudaMemsetAsync(grad + I.grad_off, 0, 3 * I.ncell * sizeof(float), s));
+        if (mt) EFM_CK(cudaMemsetAsync(mtg + (size_t)i * EFM_NSRC * 6, 0, EFM_NSRC * 6 * sizeof(double), s));
+        const int steps = (model || (flags & EFM_GRAD_NT1)) ? I.nt - 1 : I.nt;
+        maxsteps = std::max(maxsteps, steps);
+        EfmInst a = base_table(I);
+        a.nsteps = steps;
+        for (int c = 0; c < 3; ++c) a.f.v[c] = a.f.vo[c] = I.bv(c);
+        for (int c = 0; c < 6; ++c) a.f.t[c] = I.bt(c);
+        a.res = res + I.gather_off;
+        a.mtg = mt ? mtg + (size_t)i * EFM_NSRC * 6 : nullptr;
+        tab[i] = a;
+        for (int p = 0; p < 2; ++p) {
+            EfmInst r = base_table(I);
+            r.nsteps = I.nt - 1;
+            r.k = -r.k;
+            for (int c = 0; c < 3; ++c) {
+                r.f.v[c] = p == 0 ? I.va(c) : I.vb(c);
+                r.f.vo[c] = p == 0 ? I.vb(c) : I.va(c);
+                r.bv[c] = I.bv(c);
+            }
+            for (int c = 0; c < 6; ++c) {
+                r.f.t[c] = I.tt(c);
+                r.bt[c] = I.bt(c);
+            }
+            r.border = I.border;
+            if (model) {
+                r.g_lam = grad + I.grad_off;
+                r.g_mu = grad + I.grad_off + I.ncell;
+                r.g_rho = grad + I.grad_off + 2 * I.ncell;
+            }
+            tab[(size_t)(2 + p) * n + i] = r;
+        }
+    }
+    // device tables: slot 0 adjoint, slots 2 and 3 reverse rebuild (even / odd iteration)
+    EFM_CK(cudaMemcpyAsync(ctx->d_tab, tab.data(), tab.size() * sizeof(EfmInst),
+                           cudaMemcpyHostToDevice, s));
+    const EfmInst *t_adj = ctx->d_tab;
+    for (int it = 0; it < maxsteps; ++it) {
+        if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
+                 return efm_launch_stress(EFM_ADJ, t_adj, n, ctx->total_tiles, it, s);
+             })))
+            return rc;
+        if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
+                 return efm_launch_velocity(EFM_ADJ, t_adj, n, ctx->total_tiles, it, s);
+             })))
+            return rc;
+        if (model) {
+            const EfmInst *t_rev = ctx->d_tab + (size_t)(2 + (it & 1)) * n;
+            if ((rc = timed_launch(ctx, EFM_K_REV_VELOCITY, s, [&] {
+                     return efm_launch_velocity(EFM_REV, t_rev, n, ctx->total_tiles, it, s);
+                 })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_REV_STRESS, s, [&] {
+                     return efm_launch_stress(EFM_REV, t_rev, n, ctx->total_tiles, it, s);
+                 })))
+                return rc;
+        }
+    }
+    if (model)
+        for (Inst &I : ctx->inst) I.fwd_saved = false;  // the rebuild consumed the forward state
+    return EFM_OK;
+}
+
+int efm_residual_misfit(const efm_ctx *ctx_c, const float *mod, const float *obs, float *res,
+                        double *misfit, void *stream) {
+    efm_ctx *ctx = const_cast<efm_ctx *>(ctx_c);
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (!mod || !obs || !res || !misfit) return fail(EFM_ERR_ARG, "null argument");
+    const int n = (int)ctx->inst.size();
+    cudaStream_t s = (cudaStream_t)stream;
+    return timed_launch(ctx, EFM_K_REDUCE, s, [&] {
+        return efm_util_reduce(mod, obs, res, ctx->d_seg, n, 0, 0.5, ctx->d_partial,
+                               EFM_RED_BLOCKS, misfit, s);
+    });
+}
+
+int efm_set_timing(efm_ctx *ctx, int enable) {
+    if (ctx == nullptr) return fail(EFM_ERR_ARG, "null context");
+    ctx->timing = enable != 0;
+    return EFM_OK;
+}
+
+int efm_kernel_stats(efm_ctx *ctx, int64_t *launches, double *ms, int reset) {
+    if (ctx == nullptr) return fail(EFM_ERR_ARG, "null context");
+    int rc = collect_times(ctx);
+    if (rc) return rc;
+    for (int k = 0; k < EFM_NKERN; ++k) {
+        if (launches) launches[k] = ctx->launches[k];
+        if (ms) ms[k] = ctx->ms[k];
+        if (reset) {
+            ctx->launches[k] = 0;
+            ctx->ms[k] = 0.0;
+        }
+    }
+    return EFM_OK;
+}
+
+int efm_dot(const float *a, const float *b, int64_t n, double *out, void *stream) {
+    if (!a || !b || !out || n < 0) return fail(EFM_ERR_ARG, "bad argument");
+    double *partial;
+    int64_t *seg;
+    int rc = get_scratch(1, &partial, &seg);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t h[2] = {0, n};
+    EFM_CK(cudaMemcpyAsync(seg, h, sizeof(h), cudaMemcpyHostToDevice, s));
+    EFM_CK(efm_util_reduce(a, b, nullptr, seg, 1, 1, 1.0, partial, EFM_RED_BLOCKS, out, s));
+    return EFM_OK;
+}
+
+int efm_lbfgs_history(float *sk, float *yk, const float *m, const float *g, int layers, int64_t n,
+                      int iter, void *stream) {
+    if (!sk || !yk || !m || !g || layers < 2 || n < 0 || iter < 0)
+        return fail(EFM_ERR_ARG, "bad argument");
+    EFM_CK(efm_util_lbfgs_history(sk, yk, m, g, layers, n, iter, (cudaStream_t)stream));
+    return EFM_OK;
+}
+
+int efm_lbfgs_direction(const float *sk, const float *yk, const float *g, float *r, double *work,
+                        int layers, int64_t n, int iter, void *stream) {
+    if (!sk || !yk || !g || !r || !work || layers < 2 || n < 0 || iter < 0)
+        return fail(EFM_ERR_ARG, "bad argument");
+    double *partial;
+    int64_t *seg;
+    int rc = get_scratch(1, &partial, &seg);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t h[2] = {0, n};
+    EFM_CK(cudaMemcpyAsync(seg, h, sizeof(h), cudaMemcpyHostToDevice, s));
+    EFM_CK(efm_util_lbfgs_direction(sk, yk, g, r, work, layers, n, iter, partial, EFM_RED_BLOCKS,
+                                    seg, s));
+    return EFM_OK;
+}
+
+int efm_smooth_mask(float *g, float *tmp, int nx, int ny, int nz, float sigma, int lenpml, int top,
+                    void *stream) {
+    if (!g || !tmp || nx <= 0 || ny <= 0 || nz <= 0 || sigma < 0.f || sigma > 4.f)
+        return fail(EFM_ERR_ARG, "bad argument (sigma must be in [0, 4])");
+    EFM_CK(efm_util_smooth_mask(g, tmp, nx, ny, nz, sigma, lenpml, top, (cudaStream_t)stream));
+    return EFM_OK;
+}
+
+int efm_chain_rule(float *gl, float *gm, float *gr, const float *vp, const float *vs,
+                   const float *rho, int64_t n, void *stream) {
+    if (!gl || !gm || !gr || !vp || !vs || !rho || n < 0) return fail(EFM_ERR_ARG, "bad argument");
+    EFM_CK(efm_util_chain_rule(gl, gm, gr, vp, vs, rho, n, (cudaStream_t)stream));
+    return EFM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,209 @@
+/*
+ * efm.h -- C ABI of the B200-native elastic FDTD / FWI library (libefm.so).
+ *
+ * Hot path: 3-D isotropic-elastic velocity-stress staggered-grid FDTD with CPML and a
+ * moment-tensor source, the adjoint gradients for lambda/mu/rho (-> Vp/Vs/rho) and the
+ * six moment-tensor components, and the L-BFGS update of
+ * jheyston/Elastic_FM_Vp_Vs_Rho (Elastic3DGPU_MT_VP_VS_RHO_MPI/mainPropElastic3D_MT.py,
+ * lbfgs.py).  The reference has no FFI of its own: its interface is the Python driver
+ * surface (class Elastic3D, lbfgs.compute_sk_yk / L_BFGS).  Each entry point below cites
+ * the reference function(s) it replaces; the Python package
+ * elastic_fm_vp_vs_rho_b200 binds them with ctypes and exposes the reference's classes.
+ *
+ * Conventions
+ *   - Volumes are float32, C-order (ny, nz, nx): x fastest, then z (depth), y slowest,
+ *     the reference's layout (mainPropElastic3D_MT.py:72).
+ *   - Pointers named *_dev are CUDA device pointers owned by the caller (borrowed for the
+ *     duration of the call, or until replaced for model/wavelet pointers).  Pointers named
+ *     *_host are host memory read during the call.  The library allocates only its own
+ *     workspace (wavefields, compact CPML memory variables, boundary strips).
+ *   - `stream` is a cudaStream_t passed as void*; NULL means the legacy default stream.
+ *     Calls are stream-ordered; a context is not thread-safe.
+ *   - Every function returns EFM_OK (0) or an error code; efm_last_error() returns the
+ *     message of the last failure on the calling thread.  There is no CPU fallback.
+ */
+#ifndef EFM_H
+#define EFM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define EFM_API __attribute__((visibility("default")))
+#else
+#define EFM_API
+#endif
+
+#define EFM_OK 0
+#define EFM_ERR_ARG 1      /* invalid argument / shape */
+#define EFM_ERR_CUDA 2     /* CUDA runtime error */
+#define EFM_ERR_STATE 3    /* call out of order (e.g. gradient without a saved forward) */
+#define EFM_ERR_NOMEM 4    /* workspace allocation failed */
+
+#define EFM_MAX_SRC 4      /* sources per instance */
+
+/* Flags of efm_gradient(). */
+#define EFM_GRAD_MODEL 1   /* lambda/mu/rho imaging with reverse-time reconstruction */
+#define EFM_GRAD_MT 2      /* moment-tensor gradient (source-point strain) */
+#define EFM_GRAD_NT1 4     /* with EFM_GRAD_MT alone: run nt-1 adjoint steps, the loop length
+                              of backwardFields_FowardFieldsRemake (:1940) */
+
+typedef struct efm_ctx efm_ctx;
+
+/*
+ * One modelling instance: a grid + model + shot (sources, receivers, record length).
+ * Replaces the state an Elastic3D object carries (mainPropElastic3D_MT.py:1432-1466)
+ * after setModel (:2113), setStressTensor (:2109) and setIdxEarthquake (:1467-1489).
+ * Several instances (shots on one model, or different models and grid sizes) are
+ * advanced together by every call: one kernel launch per half-step covers all of them.
+ */
+typedef struct efm_instance_desc {
+    int nx, ny, nz;          /* grid (>= 2*lenpml + 4 along x and y, >= lenpml + 4 along z) */
+    int lenpml;              /* CPML width W >= 2; the top face (z < W) has no CPML */
+    float dx;                /* grid spacing used for every axis (the reference's dt/dx) */
+    float dt;                /* time step > 0 */
+    int nt;                  /* record length (time steps) */
+    const float *cpml_host;  /* ax[nx] bx[nx] ay[ny] by[ny] az[nz] bz[nz] (CPML.CPML_i, :1340-1372) */
+    const float *lam_dev;    /* lambda (ny, nz, nx) */
+    const float *mu_dev;     /* mu */
+    const float *rho_dev;    /* rho */
+    const float *wavelet_dev;/* source time function [nt] (Wavelet.ricker, :1265-1272) */
+    int nsrc;                /* 1..EFM_MAX_SRC */
+    const int *src_host;     /* [nsrc][3] cell (x, y, z) */
+    const float *mt_host;    /* [nsrc][6] Mxx Myy Mzz Mxy Mxz Myz (StressTensor, :1374-1388) */
+    int nrec;                /* >= 1 */
+    const int *rec_host;     /* [nrec][3] cell (x, y, z) (Station, :536-557) */
+} efm_instance_desc;
+
+/* Context life cycle.  Replaces module import + Elastic3D construction (:27-38, :1433). */
+EFM_API int efm_create(efm_ctx **out);
+EFM_API int efm_destroy(efm_ctx *ctx);
+EFM_API const char *efm_last_error(void);
+EFM_API int efm_version(void);
+
+/* Add an instance; returns its id (0, 1, ...) in *id.  Instances are advanced in id order. */
+EFM_API int efm_add_instance(efm_ctx *ctx, const efm_instance_desc *desc, int *id);
+/* Remove all instances and free the workspace. */
+EFM_API int efm_clear(efm_ctx *ctx);
+EFM_API int efm_num_instances(const efm_ctx *ctx);
+
+/* Replace the model pointers of one instance (Elastic3D.setModel, :2113-2120). */
+EFM_API int efm_set_model(efm_ctx *ctx, int id, const float *lam_dev, const float *mu_dev,
+                  const float *rho_dev);
+/* Replace the moment tensors of one instance (Elastic3D.setStressTensor, :2109-2111). */
+EFM_API int efm_set_moment_tensor(efm_ctx *ctx, int id, const float *mt_host);
+
+/*
+ * Number of floats of the concatenated gather buffer: for each instance in id order,
+ * [3][nt][nrec] (vx, vy, vz; time-major like Gather, :1132-1155).  Residual buffers use
+ * the same layout.  efm_gather_offset() is the float offset of one instance.
+ */
+EFM_API int64_t efm_gather_size(const efm_ctx *ctx);
+EFM_API int64_t efm_gather_offset(const efm_ctx *ctx, int id);
+/* Workspace bytes the next forward (save_borders 0/1) + gradient would allocate. */
+EFM_API int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders);
+
+/*
+ * Forward modelling of every instance (Elastic3D.forwardFields, :1812-1847 with
+ * kernel_Tau :59-128, addSource :1728-1734, kernel_Vx_Vy_Vz :133-188,
+ * kernel_get_Station :324-335 and, when save_borders, kernel_get_border :378-419).
+ * Fields start from zero.  gathers_dev: efm_gather_size() floats.
+ * save_borders = 1 keeps what efm_gradient(EFM_GRAD_MODEL) needs.
+ */
+EFM_API int efm_forward(efm_ctx *ctx, float *gathers_dev, int save_borders, void *stream);
+
+/*
+ * Adjoint pass (Elastic3D.backwardFields_FowardFieldsRemake, :1929-2054, and
+ * Elastic3D.backwardFields, :2056-2082): adjoint propagation with the residual injected
+ * into the velocities (kernel_add_adjoint_source, :310-322).
+ *   flags & EFM_GRAD_MODEL: reverse-time reconstruction of the last efm_forward(...,1)
+ *     (kernel_set_border :422-462, kernel_setZero_CPMLzone :466-499) and zero-lag imaging
+ *     (kernel_Gradients_Rho/Lambda/Mu, :191-294) for nt-1 steps; grad_dev receives, per
+ *     instance in id order, [3][ny][nz][nx] = (g_lambda, g_mu, g_rho), overwritten.
+ *   flags & EFM_GRAD_MT: source-point strain (kernel_Gradients_Mij, :337-372);
+ *     mt_grad_dev receives [ninst][EFM_MAX_SRC][6] float64, overwritten.  Over nt steps
+ *     when neither EFM_GRAD_MODEL nor EFM_GRAD_NT1 is set (backwardFields), else over the
+ *     nt-1 steps of the reconstruction loop.
+ * res_dev: residual (mod - obs) in the gather layout.
+ */
+EFM_API int efm_gradient(efm_ctx *ctx, const float *res_dev, float *grad_dev, double *mt_grad_dev,
+                 int flags, void *stream);
+
+/*
+ * Residual and misfit of every instance (computeResidual :2128-2134 and
+ * computeCostFunction :2136-2142): res = mod - obs; misfit[i] = 0.5 * sum(res^2) in
+ * float64.  All buffers in the gather layout; misfit_dev: [ninst] float64.
+ */
+EFM_API int efm_residual_misfit(const efm_ctx *ctx, const float *mod_dev, const float *obs_dev,
+                        float *res_dev, double *misfit_dev, void *stream);
+
+/* ---------------------------------------------------------------- measurement */
+
+/* Kernel kinds counted / timed per context. */
+#define EFM_K_FWD_STRESS 0
+#define EFM_K_FWD_VELOCITY 1
+#define EFM_K_ADJ_STRESS 2
+#define EFM_K_ADJ_VELOCITY 3
+#define EFM_K_REV_VELOCITY 4   /* reverse rebuild + imaging */
+#define EFM_K_REV_STRESS 5
+#define EFM_K_REDUCE 6         /* residual + misfit reduction */
+#define EFM_NKERN 7
+
+/*
+ * Record a CUDA event pair around every kernel launch of this context (enable = 1) so that
+ * efm_kernel_stats() can report per-kind device time.  No reference counterpart (the
+ * reference only prints wall-clock per FWI iteration, mainPropElastic3D_MT.py:2709).
+ */
+EFM_API int efm_set_timing(efm_ctx *ctx, int enable);
+/*
+ * Launch counts (always kept) and summed device milliseconds (when timing was on) per
+ * kernel kind since the last reset; arrays of EFM_NKERN.  Synchronizes the recorded events.
+ */
+EFM_API int efm_kernel_stats(efm_ctx *ctx, int64_t *launches, double *ms, int reset);
+
+/* ---------------------------------------------------------------- volume utilities */
+
+/* out[0] = sum(a*b) in float64 (the dot products of L_BFGS, lbfgs.py:39-65). */
+EFM_API int efm_dot(const float *a_dev, const float *b_dev, int64_t n, double *out_dev, void *stream);
+
+/*
+ * lbfgs.compute_sk_yk (lbfgs.py:12-25) on device: sk, yk are [layers][n]; layer 0 holds
+ * the current model / gradient, layers 1..layers-2 the differences (newest first).
+ */
+EFM_API int efm_lbfgs_history(float *sk_dev, float *yk_dev, const float *m_dev, const float *g_dev,
+                      int layers, int64_t n, int iter, void *stream);
+
+/*
+ * lbfgs.L_BFGS (lbfgs.py:27-67) on device: two-loop recursion r = H g with
+ * gamma = s1.y1 / y1.y1; every dot product in float64; scalars stay on the device.
+ * work_dev: at least 4 * layers + 8 doubles of scratch.
+ */
+EFM_API int efm_lbfgs_direction(const float *sk_dev, const float *yk_dev, const float *g_dev,
+                        float *r_dev, double *work_dev, int layers, int64_t n, int iter,
+                        void *stream);
+
+/*
+ * Gradient post-processing of fwi_Vp_Vs_Rho (:2479-2504): Gaussian filter (sigma, scipy
+ * 'reflect' boundaries, radius int(4 sigma + 0.5)) along all three axes, then zero
+ * z < top and the (lenpml + 2)-cell margins of the x, y and bottom faces.  In place;
+ * tmp_dev: one volume of scratch.
+ */
+EFM_API int efm_smooth_mask(float *g_dev, float *tmp_dev, int nx, int ny, int nz, float sigma,
+                    int lenpml, int top, void *stream);
+
+/*
+ * lambda/mu/rho gradients -> Vp/Vs/rho gradients for mu = rho Vs^2,
+ * lambda = rho Vp^2 - 2 mu (Model.compute_Lambda_Mu, :1196-1198); in place:
+ * g_lam -> g_vp, g_mu -> g_vs, g_rho -> g_rho at fixed Vp, Vs.
+ */
+EFM_API int efm_chain_rule(float *g_lam_dev, float *g_mu_dev, float *g_rho_dev, const float *vp_dev,
+                   const float *vs_dev, const float *rho_dev, int64_t n, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EFM_H */

@@ -1,0 +1,73 @@
+"""The two inversion drivers (fwi_Mij, fwi_Vp_Vs_Rho) against the reference's own runs.
+
+The golden runs (tests/golden/refscale.npz) executed the reference's fwi_Mij for three
+iterations and fwi_Vp_Vs_Rho for three iterations (two fixed-length steps, then an L-BFGS
+step whose backtracking ran all ten trials and reverted), with two earthquakes.
+Bounds: misfit histories 1e-4, MT histories 1e-5, final models 1e-5, smoothed gradients
+5e-4 (float32 reconstruction drift, then smoothing).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(d):
+    from elastic_fm_vp_vs_rho_b200 import CPML, Earthquake, Geometry, Model, Station, Wavelet
+    nx, ny, nz, dx = int(d["nx"]), int(d["ny"]), int(d["nz"]), float(d["dx"])
+    mt = Model(nz, ny, nx, dx, dx, dx)
+    mt.Lambda, mt.Mu, mt.Rho = d["lam_true"], d["mu_true"], d["rho_true"]
+    mt.VmaxVp = np.float32(d["vmax"])
+    m0 = Model(nz, ny, nx, dx, dx, dx)
+    m0.Lambda, m0.Mu, m0.Rho = d["lam0"], d["mu0"], d["rho0"]
+    w = Wavelet(float(d["fq"]), 14.0)
+    w.ricker()
+    cp = CPML(int(d["lenpml"]), w, mt)
+    geo = Geometry()
+    for s in d["src"]:
+        geo.addSismo(Earthquake(*[int(v) for v in s]))
+    for k in range(len(d["src"])):
+        for i in range(len(d["rec_x"])):
+            geo.sismos[k].addStation(Station(int(d["rec_x"][i]), int(d["rec_y"][i]), int(d["rec_z"][i])))
+    return mt, m0, w, cp, geo
+
+
+def test_fwi_Mij_matches_reference(golden_refscale, cuda):
+    from elastic_fm_vp_vs_rho_b200 import Elastic3D, StressTensor
+    d = golden_refscale
+    mt, m0, w, cp, geo = _setup(d)
+    e = Elastic3D(mt, geo, w, cp, mode=0)
+    e.setModel(mt)
+    e.setMode(0)
+    e.setIdxEarthquake(0)
+    e.setStressTensor(StressTensor(*d["mt_mod"]))
+    e.obsGather.Vx, e.obsGather.Vy, e.obsGather.Vz = d["obs0"]
+    hist = e.fwi_Mij(3)
+    assert rel_err(np.array(e.costFunction), d["mij_cost"]) < 1e-4
+    got = np.array([hist[c] for c in ("xx", "yy", "zz", "xy", "xz", "yz")])
+    assert rel_err(got, d["mij_hist"]) < 1e-5
+
+
+def test_fwi_Vp_Vs_Rho_matches_reference(golden_refscale, cuda):
+    from elastic_fm_vp_vs_rho_b200 import Elastic3D, Gather, StressTensor
+    d = golden_refscale
+    mt, m0, w, cp, geo = _setup(d)
+    e = Elastic3D(m0, geo, w, cp, mode=1)
+    e.setModel(m0)
+    obs = []
+    for k in range(len(d["src"])):
+        g = Gather(int(d["nt"]), len(d["rec_x"]))
+        g.Vx, g.Vy, g.Vz = d[f"obs{k}"]
+        obs.append(g)
+    cost = e.fwi_Vp_Vs_Rho(obs, [StressTensor(*d["mt_obs"])] * len(obs), 3, lbfgsLayers=4,
+                           ite_cte=2)
+    assert rel_err(np.array(cost), d["fwi_cost"]) < 1e-4
+    assert rel_err(e.mk.Lambda, d["fwi_lam"]) < 1e-5
+    assert rel_err(e.mk.Mu, d["fwi_mu"]) < 1e-5
+    assert rel_err(e.mk.Rho, d["fwi_rho"]) < 1e-5
+    gL, gM, gR = (t.cpu().numpy() for t in e.fwi_gradients)
+    assert rel_err(gL, d["fwi_glambda"]) < 5e-4
+    assert rel_err(gM, d["fwi_gmu"]) < 5e-4
+    assert rel_err(gR, d["fwi_grho"]) < 5e-4

@@ -72,6 +72,7 @@ SIGNATURES = {
     "efm_forward": (_I, [_P, _P, _I, _P]),
     "efm_gradient": (_I, [_P, _P, _P, _P, _I, _P]),
     "efm_residual_misfit": (_I, [_P, _P, _P, _P, _P, _P]),
+    "efm_residual_misfit_noalloc": (_I, [_P, _P, _P, _P, _I, _P, _P]),
     "efm_set_timing": (_I, [_P, _I]),
     "efm_kernel_stats": (_I, [_P, _P, _P, _I]),
     "efm_dot": (_I, [_P, _P, _L, _P, _P]),

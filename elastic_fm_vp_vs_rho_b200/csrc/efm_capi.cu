@@ -100,6 +100,9 @@ int get_scratch(int nseg, double **partial, int64_t **seg) {
 
 }  // namespace
 
+// Lets the library's other translation units report through efm_last_error().
+int efm_internal_fail(int code, const char *msg) { return fail(code, msg); }
+
 struct efm_ctx {
     std::vector<Inst> inst;
     EfmInst *d_tab = nullptr;  // 4 tables: FWD, ADJ, REV parity 0, REV parity 1

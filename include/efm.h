@@ -141,6 +141,34 @@ EFM_API int efm_gradient(efm_ctx *ctx, const float *res_dev, float *grad_dev, do
 EFM_API int efm_residual_misfit(const efm_ctx *ctx, const float *mod_dev, const float *obs_dev,
                         float *res_dev, double *misfit_dev, void *stream);
 
+/*
+ * The same residual and per-segment misfit as efm_residual_misfit, for callers that cannot
+ * allocate device memory.  It has no counterpart in the reference.
+ *
+ * Who needs it: an inversion driver that reserves the GPU's memory up front for its own
+ * pool (wavefields, boundary strips, L-BFGS history) and allows no further cudaMalloc, so a
+ * library call that allocates on first use would fail or break its accounting; and hosts
+ * that cannot afford cudaMalloc/cudaFree's implicit device synchronisation inside an
+ * inversion loop.  This entry point takes no context and allocates nothing: its scratch is
+ * a fixed array compiled into libefm.so (EFM_NOALLOC_MAX_SEGMENTS x 256 float64 partial
+ * sums, 128 KiB), which every GPU that loads the library holds until the process exits.
+ *
+ * seg_host: nseg + 1 non-decreasing float offsets into mod/obs/res (segment i is
+ * [seg_host[i], seg_host[i+1]), e.g. the instances of a context: efm_gather_offset);
+ * 1 <= nseg <= EFM_NOALLOC_MAX_SEGMENTS, larger nseg is rejected with EFM_ERR_ARG.
+ * misfit_dev: [nseg] float64, 0.5 * sum(res^2) per segment.
+ *
+ * The first call on each device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture.  Every call shares the array and it keeps the last call's contents (each call
+ * writes all the partials it reads, so nothing needs clearing); calls that overlap on the
+ * GPU race on it and must not be issued.
+ */
+#define EFM_NOALLOC_MAX_SEGMENTS 64
+EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_dev,
+                                        float *res_dev, const int64_t *seg_host, int nseg,
+                                        double *misfit_dev, void *stream);
+
 /* ---------------------------------------------------------------- measurement */
 
 /* Kernel kinds counted / timed per context. */

@@ -17,16 +17,20 @@ EFM_ERR_ARG = 1
 EFM_ERR_CUDA = 2
 EFM_ERR_STATE = 3
 EFM_ERR_NOMEM = 4
+EFM_ERR_TIMEOUT = 5
+EFM_OPT_STREAM_KERNELS = 1
+EFM_OPT_YCHUNK = 2
 EFM_MAX_SRC = 4
 EFM_GRAD_MODEL = 1
 EFM_GRAD_MT = 2
 EFM_GRAD_NT1 = 4
-EFM_NKERN = 7
+EFM_NKERN = 8
 KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity_imaging",
-                "rev_stress", "residual_misfit")
+                "rev_stress", "residual_misfit", "model_reciprocals")
 
 _ERRNAMES = {EFM_ERR_ARG: "EFM_ERR_ARG", EFM_ERR_CUDA: "EFM_ERR_CUDA",
-             EFM_ERR_STATE: "EFM_ERR_STATE", EFM_ERR_NOMEM: "EFM_ERR_NOMEM"}
+             EFM_ERR_STATE: "EFM_ERR_STATE", EFM_ERR_NOMEM: "EFM_ERR_NOMEM",
+             EFM_ERR_TIMEOUT: "EFM_ERR_TIMEOUT"}
 
 
 class EfmError(RuntimeError):
@@ -73,6 +77,8 @@ SIGNATURES = {
     "efm_gradient": (_I, [_P, _P, _P, _P, _I, _P]),
     "efm_residual_misfit": (_I, [_P, _P, _P, _P, _P, _P]),
     "efm_residual_misfit_noalloc": (_I, [_P, _P, _P, _P, _I, _P, _P]),
+    "efm_set_option": (_I, [_P, _I, _I]),
+    "efm_status": (_I, [_P, _P]),
     "efm_set_timing": (_I, [_P, _I]),
     "efm_kernel_stats": (_I, [_P, _P, _P, _I]),
     "efm_dot": (_I, [_P, _P, _L, _P, _P]),

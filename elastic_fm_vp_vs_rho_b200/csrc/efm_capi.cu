@@ -10,14 +10,22 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "efm.h"
 #include "efm_internal.cuh"
+#include "efm_stream.cuh"
 #include "efm_util.cuh"
 
 extern "C" cudaError_t efm_launch_stress(int pass, const EfmInst *insts, int ninst, int tiles,
                                          int it, cudaStream_t s);
 extern "C" cudaError_t efm_launch_velocity(int pass, const EfmInst *insts, int ninst, int tiles,
                                            int it, cudaStream_t s);
+extern "C" cudaError_t efm_launch_stream(int pass, int kind, const EfmInst *insts, int ninst,
+                                         int tiles, int it, cudaStream_t s);
+extern "C" cudaError_t efm_stream_init_attributes();
+extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho, float *rmu,
+                                              float *buoy, int64_t n, cudaStream_t s);
 
 namespace {
 
@@ -47,6 +55,8 @@ struct Inst {
     float *cpml = nullptr;
     uint32_t *rec_mask = nullptr;
     int *rec_lin = nullptr, *rec_id = nullptr;
+    uint8_t *rec_tile = nullptr;  // [ny][tiles_z][tiles_x] of the streaming layout
+    float *aux = nullptr;         // 1/mu, 1/rho
     float *fields = nullptr;  // va(3) t(6) | vb(3) bv(3) bt(6) when gradient-capable
     bool fields_grad = false;
     float *psi = nullptr;
@@ -119,7 +129,20 @@ struct efm_ctx {
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;       // created on demand, reused
     std::vector<std::pair<int, int>> ev_used;  // (kind, first event index) of pending pairs
+    // plane-streaming kernels
+    int opt_stream = 1;
+    int opt_ychunk = 0;
+    CUtensorMap *d_maps = nullptr;  // EFM_MAPS_PER_INST per instance
+    int maps_cap = 0;
+    unsigned int *d_err = nullptr;
+    int tiles[8] = {};              // total tiles of each table slot
 };
+
+// table slots of efm_ctx::d_tab (n entries each)
+enum { T_FWD_S, T_FWD_V, T_ADJ_S, T_ADJ_V, T_REV_V0, T_REV_V1, T_REV_S0, T_REV_S1, T_NSLOT };
+// tensor-map blocks per instance
+enum { M_FWD_S = 0, M_FWD_V = 11, M_ADJ_S = 21, M_ADJ_V = 32, M_REV_S0 = 42, M_REV_S1 = 53,
+       EFM_MAPS_PER_INST = 64 };
 
 namespace {
 
@@ -156,6 +179,98 @@ int collect_times(efm_ctx *ctx) {
     return EFM_OK;
 }
 
+// ---------------------------------------------------------------- plane-streaming support
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+cudaError_t g_encode_err = cudaSuccess;
+
+int get_encoder() {
+    std::call_once(g_encode_once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        g_encode_err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (g_encode_err == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        if (g_encode_err == cudaSuccess) g_encode_err = efm_stream_init_attributes();
+    });
+    if (g_encode == nullptr || g_encode_err != cudaSuccess)
+        return fail(EFM_ERR_CUDA, std::string("cuTensorMapEncodeTiled unavailable: ") +
+                                      cudaGetErrorString(g_encode_err));
+    return EFM_OK;
+}
+
+// 3-D map of one (ny, nz, nx) float32 volume with a (bx, bz, 1) box; out-of-range reads are 0.
+int encode_map(CUtensorMap *m, const float *base, const Inst &I, int bx, int bz) {
+    cuuint64_t dims[3] = {(cuuint64_t)I.nx, (cuuint64_t)I.nz, (cuuint64_t)I.ny};
+    cuuint64_t strides[2] = {(cuuint64_t)I.nx * 4, (cuuint64_t)I.nx * I.nz * 4};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)bz, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims,
+                          strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(EFM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return EFM_OK;
+}
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+bool stream_ok(const efm_ctx *ctx) {
+    if (!ctx->opt_stream) return false;
+    for (const auto &I : ctx->inst)
+        if (I.nx % 4 != 0 || !aligned16(I.lam) || !aligned16(I.mu) || !aligned16(I.rho)) return false;
+    return true;
+}
+
+void layout_naive(EfmInst &d) {
+    d.tiles_x = (d.nx + EFM_TX - 1) / EFM_TX;
+    d.tiles_z = (d.nz + EFM_TZ - 1) / EFM_TZ;
+    d.tiles_y = (d.ny + EFM_TY - 1) / EFM_TY;
+    d.ychunk = 0;
+}
+
+void layout_stream(EfmInst &d, int ychunk) {
+    d.tiles_x = (d.nx + EFM_STX - 1) / EFM_STX;
+    d.tiles_z = (d.nz + EFM_STZ - 1) / EFM_STZ;
+    d.ychunk = ychunk;
+    d.tiles_y = (d.ny + ychunk - 1) / ychunk;
+}
+
+// prefix tile offsets of one table; returns its total tile count
+int finish_table(EfmInst *t, int n) {
+    int tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        t[i].tile_begin = tiles;
+        tiles += t[i].tiles_x * t[i].tiles_z * t[i].tiles_y;
+    }
+    return tiles;
+}
+
+// Planes per streaming block: the chunk that fills whole waves of 3 blocks per SM best.
+int choose_ychunk(const efm_ctx *ctx) {
+    if (ctx->opt_ychunk > 0) return ctx->opt_ychunk;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const double slots = 2.0 * sms;  // two streaming blocks fit per SM
+    int best = 8;
+    double best_score = -1.0;
+    for (int yc = 4; yc <= EFM_MAX_YCHUNK; ++yc) {
+        double blocks = 0;
+        for (const auto &I : ctx->inst)
+            blocks += (double)((I.nx + EFM_STX - 1) / EFM_STX) * ((I.nz + EFM_STZ - 1) / EFM_STZ) *
+                      ((I.ny + yc - 1) / yc);
+        const double waves = std::ceil(blocks / slots);
+        const double fill = blocks / (waves * slots);
+        // full waves first; among them, longer chunks amortise the 2 extra halo planes
+        const double score = fill * (double)yc / (yc + 2.0);
+        if (score > best_score + 1e-9) {
+            best_score = score;
+            best = yc;
+        }
+    }
+    return best;
+}
+
 int64_t strip_count(const Inst &I) {
     const int64_t bx = I.nx - 2 * I.W, by = I.ny - 2 * I.W, bz = I.nz - I.W - 2;
     return 4 * by * bz + 4 * bz * bx + 4 * by * bx;
@@ -166,12 +281,16 @@ void free_inst(Inst &I) {
     cudaFree(I.rec_mask);
     cudaFree(I.rec_lin);
     cudaFree(I.rec_id);
+    cudaFree(I.rec_tile);
+    cudaFree(I.aux);
     cudaFree(I.fields);
     cudaFree(I.psi);
     cudaFree(I.border);
     I.cpml = nullptr;
     I.rec_mask = nullptr;
     I.rec_lin = I.rec_id = nullptr;
+    I.rec_tile = nullptr;
+    I.aux = nullptr;
     I.fields = I.psi = I.border = nullptr;
 }
 
@@ -203,13 +322,24 @@ int ensure_layout(efm_ctx *ctx) {
         cudaFree(ctx->d_partial);
         ctx->d_partial = nullptr;
         ctx->tab_cap = 0;
-        EFM_CK(cudaMalloc(&ctx->d_tab, 4 * (size_t)n * sizeof(EfmInst)));
+        EFM_CK(cudaMalloc(&ctx->d_tab, (size_t)T_NSLOT * n * sizeof(EfmInst)));
         EFM_CK(cudaMalloc(&ctx->d_seg, ((size_t)n + 1) * sizeof(int64_t)));
         EFM_CK(cudaMalloc(&ctx->d_partial, (size_t)n * EFM_RED_BLOCKS * sizeof(double)));
         ctx->tab_cap = n;
     }
     EFM_CK(cudaMemcpy(ctx->d_seg, ctx->seg_host.data(), (n + 1) * sizeof(int64_t),
                       cudaMemcpyHostToDevice));
+    if (ctx->d_err == nullptr) {
+        EFM_CK(cudaMalloc(&ctx->d_err, sizeof(unsigned int)));
+        EFM_CK(cudaMemset(ctx->d_err, 0, sizeof(unsigned int)));
+    }
+    if (ctx->maps_cap < n) {
+        cudaFree(ctx->d_maps);
+        ctx->d_maps = nullptr;
+        ctx->maps_cap = 0;
+        EFM_CK(cudaMalloc(&ctx->d_maps, (size_t)n * EFM_MAPS_PER_INST * sizeof(CUtensorMap)));
+        ctx->maps_cap = n;
+    }
     ctx->layout_ready = true;
     return EFM_OK;
 }
@@ -229,6 +359,12 @@ int ensure_workspace(efm_ctx *ctx, bool grad, bool borders) {
             I.fields = nf;
             I.fields_grad = grad;
             I.fwd_saved = false;
+        }
+        if (I.aux == nullptr) {
+            if (cudaMalloc(&I.aux, 2 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(EFM_ERR_NOMEM, "cannot allocate model reciprocals");
+            }
         }
         if (I.psi == nullptr) {
             const size_t np = 6 * (size_t)(I.psx_n + I.psy_n + I.psz_n);
@@ -279,6 +415,10 @@ EfmInst base_table(const Inst &I) {
         for (int c = 0; c < 6; ++c) d.mt[s][c] = I.mt[s][c];
     }
     d.wav = I.wav;
+    d.tmap = nullptr;
+    d.rmu = I.aux;
+    d.buoy = I.aux + I.ncell;
+    d.rec_tile = I.rec_tile;
     d.nrec = I.nrec;
     d.rec_mask = I.rec_mask;
     d.rec_lin = I.rec_lin;
@@ -329,6 +469,8 @@ int efm_destroy(efm_ctx *ctx) {
     if (ctx == nullptr) return EFM_OK;
     efm_clear(ctx);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    cudaFree(ctx->d_maps);
+    cudaFree(ctx->d_err);
     cudaFree(ctx->d_tab);
     cudaFree(ctx->d_seg);
     cudaFree(ctx->d_partial);
@@ -421,6 +563,16 @@ int efm_add_instance(efm_ctx *ctx, const efm_instance_desc *d, int *id) {
     if ((e = cudaMemcpy(I.rec_mask, mask.data(), mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice))) return bad(e);
     if ((e = cudaMemcpy(I.rec_lin, lin.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
     if ((e = cudaMemcpy(I.rec_id, rid.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
+    {
+        const int tx = (I.nx + EFM_STX - 1) / EFM_STX, tz = (I.nz + EFM_STZ - 1) / EFM_STZ;
+        std::vector<uint8_t> rt((size_t)I.ny * tz * tx, 0);
+        for (int r = 0; r < I.nrec; ++r) {
+            const int x = I.rec[3 * r], y = I.rec[3 * r + 1], z = I.rec[3 * r + 2];
+            rt[((size_t)y * tz + z / EFM_STZ) * tx + x / EFM_STX] = 1;
+        }
+        if ((e = cudaMalloc(&I.rec_tile, rt.size()))) return bad(e);
+        if ((e = cudaMemcpy(I.rec_tile, rt.data(), rt.size(), cudaMemcpyHostToDevice))) return bad(e);
+    }
     ctx->inst.push_back(std::move(I));
     ctx->layout_ready = false;
     if (id) *id = (int)ctx->inst.size() - 1;
@@ -466,7 +618,7 @@ int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders) {
     if (!ctx) return -1;
     int64_t b = 0;
     for (const Inst &I : ctx->inst) {
-        b += (save_borders ? 21 : 9) * I.ncell * 4;
+        b += (save_borders ? 23 : 11) * I.ncell * 4;
         b += 6 * (I.psx_n + I.psy_n + I.psz_n) * 4;
         if (save_borders) b += (int64_t)I.nt * 3 * I.strip_n * 4;
     }
@@ -480,7 +632,11 @@ int efm_forward(efm_ctx *ctx, float *gathers, int save_borders, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if ((rc = ensure_workspace(ctx, save_borders != 0, save_borders != 0))) return rc;
     const int n = (int)ctx->inst.size();
-    std::vector<EfmInst> tab(n);
+    const bool st = stream_ok(ctx);
+    if (st && (rc = get_encoder())) return rc;
+    const int yc = st ? choose_ychunk(ctx) : 0;
+    std::vector<EfmInst> tab(2 * (size_t)n);
+    std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
     int maxnt = 0;
     for (int i = 0; i < n; ++i) {
         Inst &I = ctx->inst[i];
@@ -488,22 +644,62 @@ int efm_forward(efm_ctx *ctx, float *gathers, int save_borders, void *stream) {
         if ((rc = zero_psi(I, s))) return rc;
         EfmInst d = base_table(I);
         d.nsteps = I.nt;
+        d.err = ctx->d_err;
         for (int c = 0; c < 3; ++c) d.f.v[c] = d.f.vo[c] = I.va(c);
         for (int c = 0; c < 6; ++c) d.f.t[c] = I.tt(c);
         d.gather = gathers + I.gather_off;
         d.border = save_borders ? I.border : nullptr;
-        tab[i] = d;
+        EfmInst ds = d, dv = d;
+        if (st) {
+            layout_stream(ds, yc);
+            layout_stream(dv, yc);
+            CUtensorMap *m = maps.data() + (size_t)i * EFM_MAPS_PER_INST;
+            const float *sf[11] = {I.va(0), I.va(1), I.va(2), I.aux, I.lam, I.tt(0), I.tt(1),
+                                   I.tt(2), I.tt(3), I.tt(4), I.tt(5)};
+            for (int q = 0; q < 11; ++q)
+                if ((rc = encode_map(m + M_FWD_S + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
+                                     q < 4 ? EFM_HZ : EFM_STZ)))
+                    return rc;
+            const float *vf[10] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
+                                   I.tt(1), I.va(0), I.va(1), I.va(2)};
+            for (int q = 0; q < 10; ++q)
+                if ((rc = encode_map(m + M_FWD_V + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
+                                     q < 6 ? EFM_HZ : EFM_STZ)))
+                    return rc;
+            ds.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_S;
+            dv.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_V;
+        } else {
+            layout_naive(ds);
+            layout_naive(dv);
+        }
+        tab[i] = ds;
+        tab[(size_t)n + i] = dv;
         maxnt = std::max(maxnt, I.nt);
         I.fwd_saved = false;
     }
-    EFM_CK(cudaMemcpyAsync(ctx->d_tab, tab.data(), n * sizeof(EfmInst), cudaMemcpyHostToDevice, s));
+    ctx->tiles[T_FWD_S] = finish_table(tab.data(), n);
+    ctx->tiles[T_FWD_V] = finish_table(tab.data() + n, n);
+    if (st)
+        EFM_CK(cudaMemcpyAsync(ctx->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                               cudaMemcpyHostToDevice, s));
+    EFM_CK(cudaMemcpyAsync(ctx->d_tab, tab.data(), tab.size() * sizeof(EfmInst),
+                           cudaMemcpyHostToDevice, s));
+    if (st)
+        for (const Inst &I : ctx->inst)
+            if ((rc = timed_launch(ctx, EFM_K_MODEL_AUX, s, [&] {
+                     return efm_launch_reciprocals(I.mu, I.rho, I.aux, I.aux + I.ncell, I.ncell, s);
+                 })))
+                return rc;
+    const EfmInst *ts = ctx->d_tab, *tv = ctx->d_tab + n;
     for (int it = 0; it < maxnt; ++it) {
         if ((rc = timed_launch(ctx, EFM_K_FWD_STRESS, s, [&] {
-                 return efm_launch_stress(EFM_FWD, ctx->d_tab, n, ctx->total_tiles, it, s);
+                 return st ? efm_launch_stream(EFM_FWD, 0, ts, n, ctx->tiles[T_FWD_S], it, s)
+                           : efm_launch_stress(EFM_FWD, ts, n, ctx->tiles[T_FWD_S], it, s);
              })))
             return rc;
         if ((rc = timed_launch(ctx, EFM_K_FWD_VELOCITY, s, [&] {
-                 return efm_launch_velocity(EFM_FWD, ctx->d_tab, n, ctx->total_tiles, it, s);
+                 return st ? efm_launch_stream(EFM_FWD, 1, tv, n, ctx->tiles[T_FWD_V], it, s)
+                           : efm_launch_velocity(EFM_FWD, tv, n, ctx->tiles[T_FWD_V], it, s);
              })))
             return rc;
     }
@@ -528,7 +724,12 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                             "EFM_GRAD_MODEL needs a preceding efm_forward(..., save_borders=1)");
     cudaStream_t s = (cudaStream_t)stream;
     const int n = (int)ctx->inst.size();
-    std::vector<EfmInst> tab(4 * (size_t)n);
+    const bool st = stream_ok(ctx);
+    if (st && (rc = get_encoder())) return rc;
+    const int yc = st ? choose_ychunk(ctx) : 0;
+    std::vector<EfmInst> tab((size_t)T_NSLOT * n);
+    std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
+    auto slot = [&](int k, int i) -> EfmInst & { return tab[(size_t)k * n + i]; };
     int maxsteps = 0;
     for (int i = 0; i < n; ++i) {
         Inst &I = ctx->inst[i];
@@ -538,16 +739,45 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
         if (mt) EFM_CK(cudaMemsetAsync(mtg + (size_t)i * EFM_NSRC * 6, 0, EFM_NSRC * 6 * sizeof(double), s));
         const int steps = (model || (flags & EFM_GRAD_NT1)) ? I.nt - 1 : I.nt;
         maxsteps = std::max(maxsteps, steps);
+        CUtensorMap *m = st ? maps.data() + (size_t)i * EFM_MAPS_PER_INST : nullptr;
+        const CUtensorMap *dm = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST;
+        // adjoint propagation
         EfmInst a = base_table(I);
         a.nsteps = steps;
+        a.err = ctx->d_err;
         for (int c = 0; c < 3; ++c) a.f.v[c] = a.f.vo[c] = I.bv(c);
         for (int c = 0; c < 6; ++c) a.f.t[c] = I.bt(c);
         a.res = res + I.gather_off;
         a.mtg = mt ? mtg + (size_t)i * EFM_NSRC * 6 : nullptr;
-        tab[i] = a;
+        EfmInst as = a, av = a;
+        if (st) {
+            layout_stream(as, yc);
+            layout_stream(av, yc);
+            const float *sf[11] = {I.bv(0), I.bv(1), I.bv(2), I.aux, I.lam, I.bt(0), I.bt(1),
+                                   I.bt(2), I.bt(3), I.bt(4), I.bt(5)};
+            for (int q = 0; q < 11; ++q)
+                if ((rc = encode_map(m + M_ADJ_S + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
+                                     q < 4 ? EFM_HZ : EFM_STZ)))
+                    return rc;
+            const float *vf[10] = {I.bt(0), I.bt(2), I.bt(3), I.bt(4), I.bt(5), I.aux + I.ncell,
+                                   I.bt(1), I.bv(0), I.bv(1), I.bv(2)};
+            for (int q = 0; q < 10; ++q)
+                if ((rc = encode_map(m + M_ADJ_V + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
+                                     q < 6 ? EFM_HZ : EFM_STZ)))
+                    return rc;
+            as.tmap = dm + M_ADJ_S;
+            av.tmap = dm + M_ADJ_V;
+        } else {
+            layout_naive(as);
+            layout_naive(av);
+        }
+        slot(T_ADJ_S, i) = as;
+        slot(T_ADJ_V, i) = av;
+        // reverse rebuild + imaging, even / odd iterations (ping-pong velocity buffers)
         for (int p = 0; p < 2; ++p) {
             EfmInst r = base_table(I);
             r.nsteps = I.nt - 1;
+            r.err = ctx->d_err;
             r.k = -r.k;
             for (int c = 0; c < 3; ++c) {
                 r.f.v[c] = p == 0 ? I.va(c) : I.vb(c);
@@ -564,36 +794,92 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                 r.g_mu = grad + I.grad_off + I.ncell;
                 r.g_rho = grad + I.grad_off + 2 * I.ncell;
             }
-            tab[(size_t)(2 + p) * n + i] = r;
+            EfmInst rv = r, rs = r;
+            layout_naive(rv);
+            if (st) {
+                layout_stream(rs, yc);
+                const int mb = p == 0 ? M_REV_S0 : M_REV_S1;
+                const float *sf[11] = {r.f.vo[0], r.f.vo[1], r.f.vo[2], I.aux, I.lam, I.tt(0),
+                                       I.tt(1), I.tt(2), I.tt(3), I.tt(4), I.tt(5)};
+                for (int q = 0; q < 11; ++q)
+                    if ((rc = encode_map(m + mb + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
+                                         q < 4 ? EFM_HZ : EFM_STZ)))
+                        return rc;
+                rs.tmap = dm + mb;
+            } else {
+                layout_naive(rs);
+            }
+            slot(p == 0 ? T_REV_V0 : T_REV_V1, i) = rv;
+            slot(p == 0 ? T_REV_S0 : T_REV_S1, i) = rs;
         }
     }
-    // device tables: slot 0 adjoint, slots 2 and 3 reverse rebuild (even / odd iteration)
+    for (int k = T_ADJ_S; k < T_NSLOT; ++k) ctx->tiles[k] = finish_table(&slot(k, 0), n);
+    if (st)
+        EFM_CK(cudaMemcpyAsync(ctx->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                               cudaMemcpyHostToDevice, s));
     EFM_CK(cudaMemcpyAsync(ctx->d_tab, tab.data(), tab.size() * sizeof(EfmInst),
                            cudaMemcpyHostToDevice, s));
-    const EfmInst *t_adj = ctx->d_tab;
+    if (st)
+        for (const Inst &I : ctx->inst)
+            if ((rc = timed_launch(ctx, EFM_K_MODEL_AUX, s, [&] {
+                     return efm_launch_reciprocals(I.mu, I.rho, I.aux, I.aux + I.ncell, I.ncell, s);
+                 })))
+                return rc;
+    auto dtab = [&](int k) { return (const EfmInst *)(ctx->d_tab + (size_t)k * n); };
     for (int it = 0; it < maxsteps; ++it) {
         if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
-                 return efm_launch_stress(EFM_ADJ, t_adj, n, ctx->total_tiles, it, s);
+                 return st ? efm_launch_stream(EFM_ADJ, 0, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
+                           : efm_launch_stress(EFM_ADJ, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s);
              })))
             return rc;
         if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
-                 return efm_launch_velocity(EFM_ADJ, t_adj, n, ctx->total_tiles, it, s);
+                 return st ? efm_launch_stream(EFM_ADJ, 1, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s)
+                           : efm_launch_velocity(EFM_ADJ, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s);
              })))
             return rc;
         if (model) {
-            const EfmInst *t_rev = ctx->d_tab + (size_t)(2 + (it & 1)) * n;
+            const int kv = (it & 1) ? T_REV_V1 : T_REV_V0, ks = (it & 1) ? T_REV_S1 : T_REV_S0;
             if ((rc = timed_launch(ctx, EFM_K_REV_VELOCITY, s, [&] {
-                     return efm_launch_velocity(EFM_REV, t_rev, n, ctx->total_tiles, it, s);
+                     return efm_launch_velocity(EFM_REV, dtab(kv), n, ctx->tiles[kv], it, s);
                  })))
                 return rc;
             if ((rc = timed_launch(ctx, EFM_K_REV_STRESS, s, [&] {
-                     return efm_launch_stress(EFM_REV, t_rev, n, ctx->total_tiles, it, s);
+                     return st ? efm_launch_stream(EFM_REV, 0, dtab(ks), n, ctx->tiles[ks], it, s)
+                               : efm_launch_stress(EFM_REV, dtab(ks), n, ctx->tiles[ks], it, s);
                  })))
                 return rc;
         }
     }
     if (model)
         for (Inst &I : ctx->inst) I.fwd_saved = false;  // the rebuild consumed the forward state
+    return EFM_OK;
+}
+
+int efm_set_option(efm_ctx *ctx, int option, int value) {
+    if (ctx == nullptr) return fail(EFM_ERR_ARG, "null context");
+    switch (option) {
+        case EFM_OPT_STREAM_KERNELS: ctx->opt_stream = value != 0; break;
+        case EFM_OPT_YCHUNK:
+            if (value < 0 || value > EFM_MAX_YCHUNK)
+                return fail(EFM_ERR_ARG, "ychunk must be in 0..64 (0 = automatic)");
+            ctx->opt_ychunk = value;
+            break;
+        default: return fail(EFM_ERR_ARG, "unknown option");
+    }
+    return EFM_OK;
+}
+
+int efm_status(efm_ctx *ctx, void *stream) {
+    if (ctx == nullptr) return fail(EFM_ERR_ARG, "null context");
+    if (ctx->d_err == nullptr) return EFM_OK;
+    unsigned int h = 0;
+    EFM_CK(cudaMemcpyAsync(&h, ctx->d_err, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    EFM_CK(cudaStreamSynchronize((cudaStream_t)stream));
+    if (h != 0) {
+        EFM_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(h), (cudaStream_t)stream));
+        return fail(EFM_ERR_TIMEOUT, "a kernel gave up waiting for a TMA tile (error word " +
+                                         std::to_string(h) + "); its results are invalid");
+    }
     return EFM_OK;
 }
 

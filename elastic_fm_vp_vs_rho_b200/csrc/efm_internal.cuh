@@ -3,6 +3,7 @@
 // Layout: every volume is float32 (ny, nz, nx) C-order; linear index
 // c = x + nx * (z + nz * y), the reference's `tid` (mainPropElastic3D_MT.py:72).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -30,8 +31,9 @@ struct EfmFields {
 // all instances; block b belongs to the instance with the largest tile_begin <= b.
 struct EfmInst {
     int nx, ny, nz, W;
-    int tiles_x, tiles_z, tiles_y;
+    int tiles_x, tiles_z, tiles_y;  // tile grid of the kernel family this table is built for
     int tile_begin;
+    int ychunk;        // planes per block of the plane-streaming kernels
     int nsteps;        // iterations this instance performs in the current pass
     int nt;            // record length
     float k;           // dt/dx of this pass (negative for the reverse rebuild)
@@ -62,6 +64,12 @@ struct EfmInst {
     const float *bv[3];
     const float *bt[6];
     float *g_lam, *g_mu, *g_rho;
+    // plane-streaming kernels: this pass's tensor maps, the context's error word, 1/mu and
+    // 1/rho, and a byte per (plane, tile) telling whether the tile holds a receiver
+    const CUtensorMap *tmap;
+    unsigned int *err;
+    const float *rmu, *buoy;
+    const uint8_t *rec_tile;
 };
 
 __device__ __forceinline__ int efm_find_inst(const EfmInst *__restrict__ insts, int n, int b) {

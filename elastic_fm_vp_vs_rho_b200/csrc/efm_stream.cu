@@ -1,0 +1,550 @@
+// Plane-streaming stress / velocity kernels: TMA-fed shared-memory rings.
+//
+// Each block owns a 64 x 8 (x, z) column of the grid and marches along y over a chunk of
+// planes.  One thread issues, per plane, a TMA tile load of every field the half-step reads
+// into one stage of a 4-deep ring (x/z-neighbour fields with a halo box 72 x 10 starting at
+// (x0-4, z0-1); cell-only fields with a 64 x 8 box).  While the block computes plane j from
+// the stages of planes j-1, j, j+1, plane j+2 is in flight; two blocks per SM keep ~100 KB
+// in flight without spending registers.  Each thread computes the cells (x, z) and
+// (x, z+4) of every plane.
+//
+// Per plane the compute touches no global memory it has to wait for except the compact
+// CPML memory variables of PML cells, which are requested before the stage wait.  Sources
+// and receivers are located once per block (a flag, and a bit per plane from a per-tile map
+// built on the host), reciprocals of mu and rho come precomputed, and one block barrier
+// per plane both frees the oldest stage and makes a timed-out wait end every thread's loop.
+//
+// Arithmetic, guards, CPML, sources, receivers, strips and MT strain follow efm_stencil.cu
+// (kernel_Tau :59-128, kernel_Vx_Vy_Vz :133-188 of mainPropElastic3D_MT.py); harmonic means
+// use the hardware reciprocal (relative error ~1 ulp).  Outputs are coalesced plain stores.
+#include "efm_internal.cuh"
+#include "efm_stream.cuh"
+#include "efm_tma.cuh"
+
+namespace {
+
+__device__ __forceinline__ float frcp(float a) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+
+struct Ring {
+    unsigned char *base;
+    uint64_t *bar;
+    int stage_bytes;
+    int nh;
+    int p0;  // plane held by stage 0 at its first use
+    __device__ __forceinline__ int stage(int p) const { return (p - p0) & (EFM_SR - 1); }
+    __device__ __forceinline__ uint32_t parity(int p) const { return ((p - p0) / EFM_SR) & 1; }
+    __device__ __forceinline__ const float *halo(int s, int f) const {
+        return reinterpret_cast<const float *>(base + s * stage_bytes + f * EFM_HALO_BYTES);
+    }
+    __device__ __forceinline__ const float *center(int s, int f) const {
+        return reinterpret_cast<const float *>(base + s * stage_bytes + nh * EFM_HALO_BYTES +
+                                               f * EFM_CENTER_BYTES);
+    }
+};
+
+template <int NH, int NC>
+__device__ __forceinline__ void issue_plane(const Ring &R, const CUtensorMap *tm, int x0, int z0,
+                                            int p) {
+    const int s = R.stage(p);
+    uint64_t *bar = &R.bar[s];
+    unsigned char *st = R.base + s * R.stage_bytes;
+    efm_mbar_expect_tx(bar, NH * EFM_HALO_TX + NC * EFM_CENTER_TX);
+#pragma unroll
+    for (int f = 0; f < NH; ++f)
+        efm_tma_load_3d(st + f * EFM_HALO_BYTES, tm + f, bar, x0 - EFM_HX_OFF, z0 - 1, p);
+#pragma unroll
+    for (int f = 0; f < NC; ++f)
+        efm_tma_load_3d(st + NH * EFM_HALO_BYTES + f * EFM_CENTER_BYTES, tm + NH + f, bar, x0, z0, p);
+}
+
+struct Tile {
+    int tx, tz, x0, z0, ys, ye;
+};
+
+__device__ __forceinline__ Tile stream_tile(const EfmInst &I, int block) {
+    const int lt = block - I.tile_begin;
+    Tile t;
+    t.tx = lt % I.tiles_x;
+    const int rem = lt / I.tiles_x;
+    t.tz = rem % I.tiles_z;
+    const int ty = rem / I.tiles_z;
+    t.x0 = t.tx * EFM_STX;
+    t.z0 = t.tz * EFM_STZ;
+    t.ys = ty * I.ychunk;
+    t.ye = min(I.ny, t.ys + I.ychunk);
+    return t;
+}
+
+__device__ void drain(const Ring &R, int first, int last) {
+    for (int p = first; p <= last; ++p) efm_mbar_wait(&R.bar[R.stage(p)], R.parity(p), nullptr);
+}
+
+// Block set-up shared by both kernels: barriers, prologue loads, source flag, receiver bits.
+template <int NH, int NC>
+__device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ring &R,
+                                             const CUtensorMap *tm, int *s_flags,
+                                             unsigned long long *s_recbits) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < EFM_SR; ++s) efm_mbar_init(&R.bar[s], 1);
+        efm_fence_barrier_init();
+        int f = 0;
+        for (int s = 0; s < I.nsrc; ++s)
+            if (I.sx[s] >= T.x0 && I.sx[s] < T.x0 + EFM_STX && I.sz[s] >= T.z0 &&
+                I.sz[s] < T.z0 + EFM_STZ && I.sy[s] >= T.ys && I.sy[s] < T.ye)
+                f = 1;
+        *s_flags = f;
+    }
+    if (threadIdx.x < 32) {
+        // bit q: plane ys + q holds a receiver inside this tile
+        const int l = threadIdx.x;
+        const int64_t row = (int64_t)I.tiles_z * I.tiles_x;
+        const int64_t off = (int64_t)T.tz * I.tiles_x + T.tx;
+        const bool a = T.ys + l < T.ye && I.rec_tile[(int64_t)(T.ys + l) * row + off];
+        const bool b = T.ys + 32 + l < T.ye && I.rec_tile[(int64_t)(T.ys + 32 + l) * row + off];
+        const unsigned lo = __ballot_sync(0xffffffffu, a), hi = __ballot_sync(0xffffffffu, b);
+        if (l == 0) *s_recbits = (unsigned long long)lo | ((unsigned long long)hi << 32);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NH + NC; ++q) efm_prefetch_tmap(tm + q);
+        for (int p = R.p0; p <= min(T.ye, R.p0 + EFM_SR - 1); ++p)
+            issue_plane<NH, NC>(R, tm, T.x0, T.z0, p);
+    }
+}
+
+// ------------------------------------------------------------------------------ stress
+template <int PASS>
+__device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring &R, int sm, int s0,
+                                            int sp, int it, int x, int y, int z, int hidx,
+                                            int cidx, bool has_src, const float *pp) {
+    const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+    const float *vx0 = R.halo(s0, 0), *vy0 = R.halo(s0, 1), *vz0 = R.halo(s0, 2);
+    const float *rm0 = R.halo(s0, 3), *rm1 = R.halo(sp, 3);
+    const float vxc = vx0[hidx], vyc = vy0[hidx], vzc = vz0[hidx];
+    const float dvx_dx = vxc - vx0[hidx - 1];
+    const float dvy_dy = vyc - R.halo(sm, 1)[hidx];
+    const float dvz_dz = vzc - vz0[hidx - EFM_HX];
+    const float dvx_dz = vx0[hidx + EFM_HX] - vxc;
+    const float dvx_dy = R.halo(sp, 0)[hidx] - vxc;
+    const float dvy_dx = vy0[hidx + 1] - vyc;
+    const float dvy_dz = vy0[hidx + EFM_HX] - vyc;
+    const float dvz_dx = vz0[hidx + 1] - vzc;
+    const float dvz_dy = R.halo(sp, 2)[hidx] - vzc;
+    float pvx_x = 0.f, pvy_x = 0.f, pvz_x = 0.f, pvy_y = 0.f, pvx_y = 0.f, pvz_y = 0.f;
+    float pvz_z = 0.f, pvx_z = 0.f, pvy_z = 0.f;
+    if (PASS != EFM_REV) {
+        // pp: the 9 old memory variables requested at the top of the iteration
+        if (x < W || x >= nx - W) {
+            const int xs = x < W ? x : x - (nx - 2 * W);
+            const int64_t st = (int64_t)ny * nz * 2 * W;
+            float *p = I.psi_x + ((int64_t)y * nz + z) * (2 * W) + xs;
+            const float a = I.cpml[x], b = I.cpml[nx + x];
+            pvx_x = b * pp[0] + a * dvx_dx;
+            pvy_x = b * pp[1] + a * dvy_dx;
+            pvz_x = b * pp[2] + a * dvz_dx;
+            p[0] = pvx_x;
+            p[st] = pvy_x;
+            p[2 * st] = pvz_x;
+        }
+        if (y < W || y >= ny - W) {
+            const int ys = y < W ? y : y - (ny - 2 * W);
+            const int64_t st = (int64_t)2 * W * nz * nx;
+            float *p = I.psi_y + ((int64_t)ys * nz + z) * nx + x;
+            const float a = I.cpml[2 * nx + y], b = I.cpml[2 * nx + ny + y];
+            pvy_y = b * pp[3] + a * dvy_dy;
+            pvx_y = b * pp[4] + a * dvx_dy;
+            pvz_y = b * pp[5] + a * dvz_dy;
+            p[0] = pvy_y;
+            p[st] = pvx_y;
+            p[2 * st] = pvz_y;
+        }
+        if (z >= nz - W) {
+            const int zs = z - (nz - W);
+            const int64_t st = (int64_t)ny * W * nx;
+            float *p = I.psi_z + ((int64_t)y * W + zs) * nx + x;
+            const float a = I.cpml[2 * nx + 2 * ny + z], b = I.cpml[2 * nx + 2 * ny + nz + z];
+            pvz_z = b * pp[6] + a * dvz_dz;
+            pvx_z = b * pp[7] + a * dvx_dz;
+            pvy_z = b * pp[8] + a * dvy_dz;
+            p[0] = pvz_z;
+            p[st] = pvx_z;
+            p[2 * st] = pvy_z;
+        }
+    }
+    // harmonic 4-point averages of mu from the precomputed 1/mu (:80-89)
+    const float r0 = rm0[hidx], ri = rm0[hidx + 1], rk = rm0[hidx + EFM_HX];
+    const float rik = rm0[hidx + 1 + EFM_HX];
+    const float rj = rm1[hidx], rjk = rm1[hidx + EFM_HX], rij = rm1[hidx + 1];
+    const float mu0 = frcp(r0);
+    const float mu_xz = 4.f * frcp(r0 + ri + rk + rik);
+    const float mu_xy = 4.f * frcp(r0 + ri + rj + rij);
+    const float mu_yz = 4.f * frcp(r0 + rj + rk + rjk);
+    const float lam = R.center(s0, 0)[cidx];
+    const float k = I.k;
+    const float l2m = lam + 2.f * mu0;
+    float txx = R.center(s0, 1)[cidx] + k * (l2m * (dvx_dx + pvx_x) + lam * (dvy_dy + dvz_dz + pvy_y + pvz_z));
+    float tyy = R.center(s0, 2)[cidx] + k * (l2m * (dvy_dy + pvy_y) + lam * (dvx_dx + dvz_dz + pvx_x + pvz_z));
+    float tzz = R.center(s0, 3)[cidx] + k * (l2m * (dvz_dz + pvz_z) + lam * (dvx_dx + dvy_dy + pvx_x + pvy_y));
+    float txy = R.center(s0, 4)[cidx] + k * mu_xy * ((dvx_dy + pvx_y) + (dvy_dx + pvy_x));
+    float txz = R.center(s0, 5)[cidx] + k * mu_xz * ((dvx_dz + pvx_z) + (dvz_dx + pvz_x));
+    float tyz = R.center(s0, 6)[cidx] + k * mu_yz * ((dvy_dz + pvy_z) + (dvz_dy + pvz_y));
+    if (PASS != EFM_ADJ && has_src) {
+        const int widx = (PASS == EFM_FWD) ? it : I.nt - 1 - it;
+        for (int s = 0; s < I.nsrc; ++s) {
+            if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s]) {
+                const float w = I.wav[widx];
+                const float sg = (PASS == EFM_FWD) ? 1.f : -1.f;
+                txx = __fadd_rn(txx, sg * __fmul_rn(I.mt[s][0], w));
+                tyy = __fadd_rn(tyy, sg * __fmul_rn(I.mt[s][1], w));
+                tzz = __fadd_rn(tzz, sg * __fmul_rn(I.mt[s][2], w));
+                txy = __fadd_rn(txy, sg * __fmul_rn(I.mt[s][3], w));
+                txz = __fadd_rn(txz, sg * __fmul_rn(I.mt[s][4], w));
+                tyz = __fadd_rn(tyz, sg * __fmul_rn(I.mt[s][5], w));
+            }
+        }
+    }
+    const int64_t c = x + (int64_t)nx * (z + (int64_t)nz * y);
+    I.f.t[0][c] = txx;
+    I.f.t[1][c] = tyy;
+    I.f.t[2][c] = tzz;
+    I.f.t[3][c] = txy;
+    I.f.t[4][c] = txz;
+    I.f.t[5][c] = tyz;
+    if (PASS == EFM_ADJ && has_src && I.mtg != nullptr) {
+        for (int s = 0; s < I.nsrc; ++s) {
+            if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s]) {
+                const float w = I.wav[I.nt - 1 - it];
+                const float f = __frcp_rn(2.f * mu0 * (3.f * lam + 2.f * mu0));
+                const float lpm2 = 2.f * (lam + mu0);
+                double *g = I.mtg + 6 * s;
+                g[0] += (double)(w * (f * (lpm2 * txx - lam * tyy - lam * tzz)));
+                g[1] += (double)(w * (f * (lpm2 * tyy - lam * txx - lam * tzz)));
+                g[2] += (double)(w * (f * (lpm2 * tzz - lam * txx - lam * tyy)));
+                g[3] += (double)(w * (txy * __frcp_rn(mu_xy)));
+                g[4] += (double)(w * (txz * __frcp_rn(mu_xz)));
+                g[5] += (double)(w * (tyz * __frcp_rn(mu_yz)));
+            }
+        }
+    }
+}
+
+// Request the 9 old CPML memory variables of one cell (zeros where the cell has none).
+template <int FIRST>
+__device__ __forceinline__ void load_psi(const EfmInst &I, int x, int y, int z, float *pp) {
+    const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) pp[q] = 0.f;
+    if (x < W || x >= nx - W) {
+        const int xs = x < W ? x : x - (nx - 2 * W);
+        const int64_t st = (int64_t)ny * nz * 2 * W;
+        const float *p = I.psi_x + FIRST * st + ((int64_t)y * nz + z) * (2 * W) + xs;
+        pp[0] = p[0];
+        pp[1] = p[st];
+        pp[2] = p[2 * st];
+    }
+    if (y < W || y >= ny - W) {
+        const int ys = y < W ? y : y - (ny - 2 * W);
+        const int64_t st = (int64_t)2 * W * nz * nx;
+        const float *p = I.psi_y + FIRST * st + ((int64_t)ys * nz + z) * nx + x;
+        pp[3] = p[0];
+        pp[4] = p[st];
+        pp[5] = p[2 * st];
+    }
+    if (z >= nz - W) {
+        const int zs = z - (nz - W);
+        const int64_t st = (int64_t)ny * W * nx;
+        const float *p = I.psi_z + FIRST * st + ((int64_t)y * W + zs) * nx + x;
+        pp[6] = p[0];
+        pp[7] = p[st];
+        pp[8] = p[2 * st];
+    }
+}
+
+}  // namespace
+
+// halo fields: vx vy vz 1/mu ; center fields: lambda txx tyy tzz txy txz tyz
+template <int PASS>
+__global__ void __launch_bounds__(EFM_STHREADS, 2)
+efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
+    constexpr int NH = 4, NC = 7;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t bars[EFM_SR];
+    __shared__ int s_src;
+    __shared__ unsigned long long s_rec;
+    const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
+    if (it >= I.nsteps) return;
+    const Tile T = stream_tile(I, blockIdx.x);
+    const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+    const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
+    const int x = T.x0 + lx;
+    const CUtensorMap *tm = I.tmap;
+    Ring R{smem, bars, NH * EFM_HALO_BYTES + NC * EFM_CENTER_BYTES, NH, T.ys - 1};
+    stream_setup<NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    const bool has_src = s_src != 0;
+    bool colin[2];
+    int hidx[2], cidx[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int lz = lr + 4 * h, z = T.z0 + lz;
+        hidx[h] = (lz + 1) * EFM_HX + lx + EFM_HX_OFF;
+        cidx[h] = lz * EFM_STX + lx;
+        colin[h] = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS &&
+                   !(PASS == EFM_REV && (x < W || x >= nx - W || z >= nz - W));
+    }
+    const int last = T.ye;
+    int issued_hi = min(last, R.p0 + EFM_SR - 1);
+    bool ok;
+    {
+        const bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), I.err) &&
+                          efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), I.err);
+        ok = __syncthreads_and(mine) != 0;
+    }
+    for (int j = T.ys; j < T.ye && ok; ++j) {
+        const bool plane_in = j >= EFM_HS && j < ny - EFM_HS && !(PASS == EFM_REV && (j < W || j >= ny - W));
+        float pp[2][9];
+        if (PASS != EFM_REV) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (plane_in && colin[h]) load_psi<0>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
+        }
+        const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+        if (mine && plane_in) {
+            const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (colin[h])
+                    stress_cell<PASS>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, hidx[h],
+                                      cidx[h], has_src, pp[h]);
+        }
+        ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
+        if (!ok) break;
+        if (j - 1 + EFM_SR <= last) {
+            if (threadIdx.x == 0) issue_plane<NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
+            issued_hi = j - 1 + EFM_SR;
+        }
+    }
+    if (!ok) drain(R, R.p0, issued_hi);  // no load may still target this block's smem
+}
+
+// halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint)
+template <int PASS>
+__global__ void __launch_bounds__(EFM_STHREADS, 2)
+efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
+    constexpr int NH = 6, NC = 4;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t bars[EFM_SR];
+    __shared__ int s_src;
+    __shared__ unsigned long long s_rec;
+    const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
+    if (it >= I.nsteps) return;
+    const Tile T = stream_tile(I, blockIdx.x);
+    const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+    const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
+    const int x = T.x0 + lx;
+    const CUtensorMap *tm = I.tmap;
+    Ring R{smem, bars, NH * EFM_HALO_BYTES + NC * EFM_CENTER_BYTES, NH, T.ys - 1};
+    stream_setup<NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    const unsigned long long recbits = s_rec;
+    bool colin[2], colgrid[2];
+    int hidx[2], cidx[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int lz = lr + 4 * h, z = T.z0 + lz;
+        hidx[h] = (lz + 1) * EFM_HX + lx + EFM_HX_OFF;
+        cidx[h] = lz * EFM_STX + lx;
+        colin[h] = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS;
+        colgrid[h] = x < nx && z < nz;
+    }
+    const int last = T.ye;
+    int issued_hi = min(last, R.p0 + EFM_SR - 1);
+    bool ok;
+    {
+        bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), I.err) &&
+                    efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), I.err);
+        ok = __syncthreads_and(mine) != 0;
+    }
+    const int64_t SZ = nx, SY = (int64_t)nx * nz;
+    for (int j = T.ys; j < T.ye && ok; ++j) {
+        const int y = j;
+        const bool plane_in = j >= EFM_HS && j < ny - EFM_HS;
+        const bool rec_plane = (recbits >> (j - T.ys)) & 1ull;
+        float pp[2][9];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (plane_in && colin[h]) load_psi<3>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
+        const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+        if (mine) {
+            const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int z = T.z0 + lr + 4 * h;
+                const bool guard = plane_in && colin[h];
+                const bool rec = rec_plane && colgrid[h] && efm_rec_bit(I, x, y, z);
+                if (!(guard || rec)) continue;
+                const int hi = hidx[h], ci = cidx[h];
+                const int64_t c = x + SZ * z + SY * y;
+                float nvx = R.center(s0, 1)[ci];
+                float nvy = R.center(s0, 2)[ci];
+                float nvz = R.center(s0, 3)[ci];
+                if (guard) {
+                    const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
+                    const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
+                    const float dtxx_dx = t0[hi + 1] - t0[hi];
+                    const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
+                    const float dtyy_dy = R.center(sp, 0)[ci] - R.center(s0, 0)[ci];
+                    const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
+                    const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
+                    const float dtxy_dx = txyc - t3[hi - 1];
+                    const float dtxz_dz = txzc - t4[hi - EFM_HX];
+                    const float dtxz_dx = txzc - t4[hi - 1];
+                    const float dtyz_dz = tyzc - t5[hi - EFM_HX];
+                    const float dtyz_dy = tyzc - R.halo(sm, 4)[hi];
+                    const float *p9 = pp[h];
+                    float q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f,
+                          q8 = 0.f, q9 = 0.f;
+                    if (x < W || x >= nx - W) {
+                        const int xs = x < W ? x : x - (nx - 2 * W);
+                        const int64_t st = (int64_t)ny * nz * 2 * W;
+                        float *p = I.psi_x + 3 * st + ((int64_t)y * nz + z) * (2 * W) + xs;
+                        const float a = I.cpml[x], b = I.cpml[nx + x];
+                        q1 = b * p9[0] + a * dtxx_dx;
+                        q2 = b * p9[1] + a * dtxy_dx;
+                        q3 = b * p9[2] + a * dtxz_dx;
+                        p[0] = q1;
+                        p[st] = q2;
+                        p[2 * st] = q3;
+                    }
+                    if (y < W || y >= ny - W) {
+                        const int ys = y < W ? y : y - (ny - 2 * W);
+                        const int64_t st = (int64_t)2 * W * nz * nx;
+                        float *p = I.psi_y + 3 * st + ((int64_t)ys * nz + z) * nx + x;
+                        const float a = I.cpml[2 * nx + y], b = I.cpml[2 * nx + ny + y];
+                        q4 = b * p9[3] + a * dtyy_dy;
+                        q5 = b * p9[4] + a * dtxy_dy;
+                        q6 = b * p9[5] + a * dtyz_dy;
+                        p[0] = q4;
+                        p[st] = q5;
+                        p[2 * st] = q6;
+                    }
+                    if (z >= nz - W) {
+                        const int zs = z - (nz - W);
+                        const int64_t st = (int64_t)ny * W * nx;
+                        float *p = I.psi_z + 3 * st + ((int64_t)y * W + zs) * nx + x;
+                        const float a = I.cpml[2 * nx + 2 * ny + z], b = I.cpml[2 * nx + 2 * ny + nz + z];
+                        q7 = b * p9[6] + a * dtzz_dz;
+                        q8 = b * p9[7] + a * dtxz_dz;
+                        q9 = b * p9[8] + a * dtyz_dz;
+                        p[0] = q7;
+                        p[st] = q8;
+                        p[2 * st] = q9;
+                    }
+                    // harmonic 2-point buoyancy from the precomputed 1/rho (:153-159)
+                    const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];
+                    const float bj = R.halo(sp, 5)[hi];
+                    const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
+                    const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
+                    const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
+                    const float k = I.k;
+                    nvx = nvx + k * b_x * ((dtxx_dx + q1) + (dtxy_dy + q5) + (dtxz_dz + q8));
+                    nvy = nvy + k * b_y * ((dtxy_dx + q2) + (dtyy_dy + q4) + (dtyz_dz + q9));
+                    nvz = nvz + k * b_z * ((dtxz_dx + q3) + (dtyz_dy + q6) + (dtzz_dz + q7));
+                }
+                if (PASS == EFM_ADJ && rec) {
+                    const int tr = I.nt - 1 - it;
+                    const int64_t ntr = (int64_t)I.nt * I.nrec;
+                    for (int q = efm_rec_find(I, (int)c); q >= 0 && q < I.nrec && I.rec_lin[q] == (int)c; ++q) {
+                        const int64_t o = (int64_t)tr * I.nrec + I.rec_id[q];
+                        nvx = __fadd_rn(nvx, I.res[o]);
+                        nvy = __fadd_rn(nvy, I.res[ntr + o]);
+                        nvz = __fadd_rn(nvz, I.res[2 * ntr + o]);
+                    }
+                }
+                I.f.v[0][c] = nvx;
+                I.f.v[1][c] = nvy;
+                I.f.v[2][c] = nvz;
+                if (PASS == EFM_FWD) {
+                    if (rec && I.gather != nullptr) {
+                        const int64_t ntr = (int64_t)I.nt * I.nrec;
+                        for (int q = efm_rec_find(I, (int)c); q >= 0 && q < I.nrec && I.rec_lin[q] == (int)c; ++q) {
+                            const int64_t o = (int64_t)it * I.nrec + I.rec_id[q];
+                            I.gather[o] = nvx;
+                            I.gather[ntr + o] = nvy;
+                            I.gather[2 * ntr + o] = nvz;
+                        }
+                    }
+                    if (I.border != nullptr) {
+                        int64_t slot[3];
+                        const int nslot = efm_strip_slots(I, x, y, z, slot);
+                        float *s = I.border + (int64_t)it * 3 * I.strip_n;
+                        for (int q = 0; q < nslot; ++q) {
+                            s[slot[q]] = nvx;
+                            s[I.strip_n + slot[q]] = nvy;
+                            s[2 * I.strip_n + slot[q]] = nvz;
+                        }
+                    }
+                }
+            }
+        }
+        ok = __syncthreads_and(mine) != 0;
+        if (!ok) break;
+        if (j - 1 + EFM_SR <= last) {
+            if (threadIdx.x == 0) issue_plane<NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
+            issued_hi = j - 1 + EFM_SR;
+        }
+    }
+    if (!ok) drain(R, R.p0, issued_hi);
+}
+
+// 1/mu and 1/rho for the streaming kernels (once per call; the model may change in place).
+__global__ void efm_model_reciprocals(const float *__restrict__ mu, const float *__restrict__ rho,
+                                      float *__restrict__ rmu, float *__restrict__ buoy, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        rmu[i] = __frcp_rn(mu[i]);
+        buoy[i] = __frcp_rn(rho[i]);
+    }
+}
+
+// ---------------------------------------------------------------------------- launchers
+static const size_t kSmemStress = (size_t)EFM_SR * (4 * EFM_HALO_BYTES + 7 * EFM_CENTER_BYTES);
+static const size_t kSmemVelocity = (size_t)EFM_SR * (6 * EFM_HALO_BYTES + 4 * EFM_CENTER_BYTES);
+
+extern "C" cudaError_t efm_launch_stream(int pass, int kind, const EfmInst *insts, int ninst,
+                                         int tiles, int it, cudaStream_t s) {
+    if (kind == 0) {
+        switch (pass) {
+            case EFM_FWD: efm_stress_stream<EFM_FWD><<<tiles, EFM_STHREADS, kSmemStress, s>>>(insts, ninst, it); break;
+            case EFM_ADJ: efm_stress_stream<EFM_ADJ><<<tiles, EFM_STHREADS, kSmemStress, s>>>(insts, ninst, it); break;
+            default: efm_stress_stream<EFM_REV><<<tiles, EFM_STHREADS, kSmemStress, s>>>(insts, ninst, it); break;
+        }
+    } else {
+        switch (pass) {
+            case EFM_FWD: efm_velocity_stream<EFM_FWD><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
+            default: efm_velocity_stream<EFM_ADJ><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
+        }
+    }
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho, float *rmu,
+                                              float *buoy, int64_t n, cudaStream_t s) {
+    int64_t b = (n + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    efm_model_reciprocals<<<(int)b, 256, 0, s>>>(mu, rho, rmu, buoy, n);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t efm_stream_init_attributes() {
+    cudaError_t e;
+    const int ss = (int)kSmemStress, sv = (int)kSmemVelocity;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_REV>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+    return cudaSuccess;
+}

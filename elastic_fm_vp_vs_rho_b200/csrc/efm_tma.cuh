@@ -1,0 +1,67 @@
+// Thin inline-PTX layer for the plane-streaming kernels: mbarriers and TMA tile loads.
+//
+// Only plain (non-multicast) cp.async.bulk.tensor loads from this GPU's own memory are
+// issued.  Every mbarrier wait is bounded: after EFM_WAIT_LIMIT polls it gives up, sets the
+// context's error word and lets the caller drain and return, so a lost transfer reports an
+// error instead of hanging the GPU.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define EFM_WAIT_LIMIT (1u << 22)
+#define EFM_ERR_FLAG_TIMEOUT 1u
+
+__device__ __forceinline__ uint32_t efm_smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void efm_mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(efm_smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void efm_fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void efm_mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(efm_smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool efm_mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(efm_smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of `bar`; false after EFM_WAIT_LIMIT polls (error flag set).
+__device__ __forceinline__ bool efm_mbar_wait(uint64_t *bar, uint32_t parity,
+                                              unsigned int *err_flag) {
+    for (uint32_t i = 0; i < EFM_WAIT_LIMIT; ++i)
+        if (efm_mbar_try_wait(bar, parity)) return true;
+    if (err_flag) atomicOr(err_flag, EFM_ERR_FLAG_TIMEOUT);
+    return false;
+}
+
+__device__ __forceinline__ void efm_prefetch_tmap(const CUtensorMap *m) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(m) : "memory");
+}
+
+// 3-D tile load (x, z, y coordinates, x innermost) into shared memory, completing on `bar`.
+__device__ __forceinline__ void efm_tma_load_3d(void *dst, const CUtensorMap *m, uint64_t *bar,
+                                                int x, int z, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(efm_smem_addr(dst)),
+        "l"(m), "r"(efm_smem_addr(bar)), "r"(x), "r"(z), "r"(y)
+        : "memory");
+}

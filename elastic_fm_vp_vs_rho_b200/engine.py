@@ -130,6 +130,14 @@ class ShotBatch:
         check(self._L.efm_set_model(self._ctx, i, ptr(lam), ptr(mu), ptr(rho)))
         self._keep[i].update(lam=lam, mu=mu, rho=rho)
 
+    def set_option(self, option, value):
+        """efm_set_option: _lib.EFM_OPT_STREAM_KERNELS (1/0) or _lib.EFM_OPT_YCHUNK (planes)."""
+        check(self._L.efm_set_option(self._ctx, int(option), int(value)))
+
+    def status(self, stream=None):
+        """Raise EfmError(EFM_ERR_TIMEOUT) if a kernel gave up a bounded wait (synchronizes)."""
+        check(self._L.efm_status(self._ctx, stream_ptr(stream)))
+
     def set_moment_tensor(self, i, mt):
         a = np.ascontiguousarray(np.asarray(mt, np.float32).reshape(-1, 6))
         if len(a) != self.infos[i].nsrc:

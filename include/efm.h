@@ -43,6 +43,7 @@ extern "C" {
 #define EFM_ERR_CUDA 2     /* CUDA runtime error */
 #define EFM_ERR_STATE 3    /* call out of order (e.g. gradient without a saved forward) */
 #define EFM_ERR_NOMEM 4    /* workspace allocation failed */
+#define EFM_ERR_TIMEOUT 5  /* a kernel gave up waiting for a shared-memory tile (efm_status) */
 
 #define EFM_MAX_SRC 4      /* sources per instance */
 
@@ -169,6 +170,22 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
                                         float *res_dev, const int64_t *seg_host, int nseg,
                                         double *misfit_dev, void *stream);
 
+/* ---------------------------------------------------------------- options */
+
+/* 1 (default): TMA plane-streaming stencil kernels wherever every instance allows them
+ * (nx a multiple of 4, 16-byte aligned model pointers); 0: one-thread-per-cell kernels. */
+#define EFM_OPT_STREAM_KERNELS 1
+/* Planes per block of the plane-streaming kernels; 0 (default) picks the chunk that fills
+ * whole waves of blocks best. */
+#define EFM_OPT_YCHUNK 2
+EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
+
+/*
+ * Synchronizes `stream` and returns EFM_ERR_TIMEOUT if a kernel of this context gave up a
+ * bounded wait for a tile since the last check (its outputs are then invalid), else EFM_OK.
+ */
+EFM_API int efm_status(efm_ctx *ctx, void *stream);
+
 /* ---------------------------------------------------------------- measurement */
 
 /* Kernel kinds counted / timed per context. */
@@ -179,7 +196,8 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 #define EFM_K_REV_VELOCITY 4   /* reverse rebuild + imaging */
 #define EFM_K_REV_STRESS 5
 #define EFM_K_REDUCE 6         /* residual + misfit reduction */
-#define EFM_NKERN 7
+#define EFM_K_MODEL_AUX 7      /* 1/mu, 1/rho for the plane-streaming kernels (once per call) */
+#define EFM_NKERN 8
 
 /*
  * Record a CUDA event pair around every kernel launch of this context (enable = 1) so that

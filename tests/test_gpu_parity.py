@@ -289,3 +289,27 @@ def test_receivers_on_never_updated_cells(golden_c1scale, cuda):
     gm = O.mt_gradient(d["lam_true"], d["mu_true"], d["rho_true"], cp, d["waveform"][:nt],
                        float(d["dt"]), float(d["dx"]), tuple(d["src"][0]), rtuple, res)
     assert rel_err(m[0, 0].cpu().numpy(), gm) < TOL_MT
+
+
+@pytest.mark.parametrize("ychunk", [0, 5, 64])
+def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychunk):
+    """TMA plane-streaming kernels = one-thread-per-cell kernels (same arithmetic up to the
+    hardware reciprocal in the harmonic means), for the forward, the adjoint, the reverse
+    rebuild and the MT gradient; several chunk lengths."""
+    from elastic_fm_vp_vs_rho_b200 import _lib
+    d = golden_c1scale
+    out = []
+    for stream in (1, 0):
+        b = _batch(d, d["lam0"], d["mu0"], d["rho0"], d["mt_obs"])
+        b.set_option(_lib.EFM_OPT_STREAM_KERNELS, stream)
+        b.set_option(_lib.EFM_OPT_YCHUNK, ychunk)
+        mod = b.forward(save_borders=True)
+        res, _ = b.residual_misfit(mod, cuda.as_tensor(d["obs0"].reshape(-1)).cuda())
+        g, m = b.gradient(res, model=True, mt=True)
+        b.status()
+        out.append((mod.cpu().numpy(), b.grad_view(g, 0).cpu().numpy(), m.cpu().numpy()))
+    (m1, g1, t1), (m2, g2, t2) = out
+    assert rel_err(m1, m2) < 1e-5
+    for i in range(3):
+        assert rel_err(g1[i], g2[i]) < 5e-5
+    assert rel_err(t1, t2) < 2e-5

@@ -88,8 +88,10 @@ def algorithmic_bytes(w):
     stress:   V(3) + tau(6) + lambda, mu read, tau(6) written = 68 B/cell, plus 24 B per
               cell and active CPML direction (3 memory variables read + written);
     velocity: tau(6) + V(3) + rho read, V(3) written = 52 B/cell + 24 B per CPML direction;
-    reverse velocity + imaging: tau(6), V_old(3), rho, adjoint V(3) and tau(6), lambda, mu,
-              3 gradients read; V_new(3) and 3 gradients written = 120 B/cell;
+    reverse velocity: tau(6), V_old(3), 1/rho read, V_new(3) written = 52 B/cell (the
+              one-thread-per-cell kernel also images: 120 B/cell, see imaging);
+    imaging: fV_present(3), fV(3), adjoint V(3) and tau(6), lambda, 1/mu, 3 gradients read,
+              3 gradients written = 92 B/cell;
     reverse stress: 68 B per cell of the non-CPML box;
     misfit: 3 * nt * nrec * 12 B."""
     nx, ny, nz, W = w.nx, w.ny, w.nz, w.lenpml
@@ -102,7 +104,8 @@ def algorithmic_bytes(w):
         "fwd_velocity": 52 * n + 24 * pml_dirs,
         "adj_stress": 68 * n + 24 * pml_dirs,
         "adj_velocity": 52 * n + 24 * pml_dirs,
-        "rev_velocity_imaging": 120 * n,
+        "rev_velocity": 52 * n,
+        "imaging": 92 * n,
         "rev_stress": 68 * box,
         "residual_misfit": 12 * ntr,
         "model_reciprocals": 16 * n,

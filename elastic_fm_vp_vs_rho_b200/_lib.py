@@ -24,9 +24,9 @@ EFM_MAX_SRC = 4
 EFM_GRAD_MODEL = 1
 EFM_GRAD_MT = 2
 EFM_GRAD_NT1 = 4
-EFM_NKERN = 8
-KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity_imaging",
-                "rev_stress", "residual_misfit", "model_reciprocals")
+EFM_NKERN = 9
+KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity",
+                "rev_stress", "residual_misfit", "model_reciprocals", "imaging")
 
 _ERRNAMES = {EFM_ERR_ARG: "EFM_ERR_ARG", EFM_ERR_CUDA: "EFM_ERR_CUDA",
              EFM_ERR_STATE: "EFM_ERR_STATE", EFM_ERR_NOMEM: "EFM_ERR_NOMEM",

@@ -24,6 +24,8 @@ extern "C" cudaError_t efm_launch_velocity(int pass, const EfmInst *insts, int n
 extern "C" cudaError_t efm_launch_stream(int pass, int kind, const EfmInst *insts, int ninst,
                                          int tiles, int it, cudaStream_t s);
 extern "C" cudaError_t efm_stream_init_attributes();
+extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int tiles, int it,
+                                        cudaStream_t s);
 extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho, float *rmu,
                                               float *buoy, int64_t n, cudaStream_t s);
 
@@ -135,14 +137,17 @@ struct efm_ctx {
     CUtensorMap *d_maps = nullptr;  // EFM_MAPS_PER_INST per instance
     int maps_cap = 0;
     unsigned int *d_err = nullptr;
-    int tiles[8] = {};              // total tiles of each table slot
+    int tiles[16] = {};             // total tiles of each table slot (T_NSLOT <= 16)
 };
 
 // table slots of efm_ctx::d_tab (n entries each)
-enum { T_FWD_S, T_FWD_V, T_ADJ_S, T_ADJ_V, T_REV_V0, T_REV_V1, T_REV_S0, T_REV_S1, T_NSLOT };
+enum { T_FWD_S, T_FWD_V, T_ADJ_S, T_ADJ_V, T_REV_V0, T_REV_V1, T_REV_S0, T_REV_S1, T_IMG0,
+       T_IMG1, T_NSLOT };
 // tensor-map blocks per instance
 enum { M_FWD_S = 0, M_FWD_V = 11, M_ADJ_S = 21, M_ADJ_V = 32, M_REV_S0 = 42, M_REV_S1 = 53,
-       EFM_MAPS_PER_INST = 64 };
+       M_REV_V0 = 64, M_REV_V1 = 74, M_IMG0 = 84, M_IMG1 = 104, EFM_MAPS_PER_INST = 128 };
+#define EFM_IMG_TZ 4
+static_assert(T_NSLOT <= 16, "efm_ctx::tiles holds 16 table slots");
 
 namespace {
 
@@ -228,9 +233,9 @@ void layout_naive(EfmInst &d) {
     d.ychunk = 0;
 }
 
-void layout_stream(EfmInst &d, int ychunk) {
+void layout_stream(EfmInst &d, int ychunk, int tz = EFM_STZ) {
     d.tiles_x = (d.nx + EFM_STX - 1) / EFM_STX;
-    d.tiles_z = (d.nz + EFM_STZ - 1) / EFM_STZ;
+    d.tiles_z = (d.nz + tz - 1) / tz;
     d.ychunk = ychunk;
     d.tiles_y = (d.ny + ychunk - 1) / ychunk;
 }
@@ -245,19 +250,20 @@ int finish_table(EfmInst *t, int n) {
     return tiles;
 }
 
-// Planes per streaming block: the chunk that fills whole waves of 3 blocks per SM best.
-int choose_ychunk(const efm_ctx *ctx) {
+// Planes per streaming block: the chunk that fills whole waves of blocks best, for tiles of
+// EFM_STX x tz cells and `per_sm` resident blocks per SM.
+int choose_ychunk(const efm_ctx *ctx, int tz = EFM_STZ, int per_sm = 2) {
     if (ctx->opt_ychunk > 0) return ctx->opt_ychunk;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const double slots = 2.0 * sms;  // two streaming blocks fit per SM
+    const double slots = (double)per_sm * sms;
     int best = 8;
     double best_score = -1.0;
     for (int yc = 4; yc <= EFM_MAX_YCHUNK; ++yc) {
         double blocks = 0;
         for (const auto &I : ctx->inst)
-            blocks += (double)((I.nx + EFM_STX - 1) / EFM_STX) * ((I.nz + EFM_STZ - 1) / EFM_STZ) *
+            blocks += (double)((I.nx + EFM_STX - 1) / EFM_STX) * ((I.nz + tz - 1) / tz) *
                       ((I.ny + yc - 1) / yc);
         const double waves = std::ceil(blocks / slots);
         const double fill = blocks / (waves * slots);
@@ -727,6 +733,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     const bool st = stream_ok(ctx);
     if (st && (rc = get_encoder())) return rc;
     const int yc = st ? choose_ychunk(ctx) : 0;
+    const int yci = st ? choose_ychunk(ctx, EFM_IMG_TZ, 3) : 0;
     std::vector<EfmInst> tab((size_t)T_NSLOT * n);
     std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
     auto slot = [&](int k, int i) -> EfmInst & { return tab[(size_t)k * n + i]; };
@@ -794,8 +801,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                 r.g_mu = grad + I.grad_off + I.ncell;
                 r.g_rho = grad + I.grad_off + 2 * I.ncell;
             }
-            EfmInst rv = r, rs = r;
-            layout_naive(rv);
+            EfmInst rv = r, rs = r, ri = r;
             if (st) {
                 layout_stream(rs, yc);
                 const int mb = p == 0 ? M_REV_S0 : M_REV_S1;
@@ -806,11 +812,40 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                                          q < 4 ? EFM_HZ : EFM_STZ)))
                         return rc;
                 rs.tmap = dm + mb;
+                // reverse velocity rebuild: the velocity pass's fields, old velocity in f.v
+                layout_stream(rv, yc);
+                const int mv = p == 0 ? M_REV_V0 : M_REV_V1;
+                const float *vf[10] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
+                                       I.tt(1), r.f.v[0], r.f.v[1], r.f.v[2]};
+                for (int q = 0; q < 10; ++q)
+                    if ((rc = encode_map(m + mv + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
+                                         q < 6 ? EFM_HZ : EFM_STZ)))
+                        return rc;
+                rv.tmap = dm + mv;
+                // imaging: halo fV_present + 1/mu (72 x 7 from z0-2), cells 64 x 4
+                if (model) {
+                    layout_stream(ri, yci, EFM_IMG_TZ);
+                    const int mi = p == 0 ? M_IMG0 : M_IMG1;
+                    const float *hf[4] = {r.f.v[0], r.f.v[1], r.f.v[2], I.aux};
+                    for (int q = 0; q < 4; ++q)
+                        if ((rc = encode_map(m + mi + q, hf[q], I, EFM_HX, EFM_IMG_TZ + 3))) return rc;
+                    const float *cf[16] = {r.f.vo[0], r.f.vo[1], r.f.vo[2], I.bv(0), I.bv(1), I.bv(2),
+                                           I.bt(0), I.bt(1), I.bt(2), I.bt(3), I.bt(4), I.bt(5),
+                                           I.lam, r.g_lam, r.g_mu, r.g_rho};
+                    for (int q = 0; q < 16; ++q)
+                        if ((rc = encode_map(m + mi + 4 + q, cf[q], I, EFM_STX, EFM_IMG_TZ))) return rc;
+                    ri.tmap = dm + mi;
+                } else {
+                    layout_stream(ri, yci, EFM_IMG_TZ);
+                }
             } else {
                 layout_naive(rs);
+                layout_naive(rv);
+                layout_naive(ri);
             }
             slot(p == 0 ? T_REV_V0 : T_REV_V1, i) = rv;
             slot(p == 0 ? T_REV_S0 : T_REV_S1, i) = rs;
+            slot(p == 0 ? T_IMG0 : T_IMG1, i) = ri;
         }
     }
     for (int k = T_ADJ_S; k < T_NSLOT; ++k) ctx->tiles[k] = finish_table(&slot(k, 0), n);
@@ -839,9 +874,16 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
             return rc;
         if (model) {
             const int kv = (it & 1) ? T_REV_V1 : T_REV_V0, ks = (it & 1) ? T_REV_S1 : T_REV_S0;
+            const int ki = (it & 1) ? T_IMG1 : T_IMG0;
+            // stream kernels: rebuild, then imaging; otherwise one fused rebuild + imaging kernel
             if ((rc = timed_launch(ctx, EFM_K_REV_VELOCITY, s, [&] {
-                     return efm_launch_velocity(EFM_REV, dtab(kv), n, ctx->tiles[kv], it, s);
+                     return st ? efm_launch_stream(EFM_REV, 1, dtab(kv), n, ctx->tiles[kv], it, s)
+                               : efm_launch_velocity(EFM_REV, dtab(kv), n, ctx->tiles[kv], it, s);
                  })))
+                return rc;
+            if (st && (rc = timed_launch(ctx, EFM_K_IMAGING, s, [&] {
+                           return efm_launch_image(dtab(ki), n, ctx->tiles[ki], it, s);
+                       })))
                 return rc;
             if ((rc = timed_launch(ctx, EFM_K_REV_STRESS, s, [&] {
                      return st ? efm_launch_stream(EFM_REV, 0, dtab(ks), n, ctx->tiles[ks], it, s)

@@ -373,11 +373,60 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         const bool plane_in = j >= EFM_HS && j < ny - EFM_HS;
         const bool rec_plane = (recbits >> (j - T.ys)) & 1ull;
         float pp[2][9];
+        if (PASS != EFM_REV) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-            if (plane_in && colin[h]) load_psi<3>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
+            for (int h = 0; h < 2; ++h)
+                if (plane_in && colin[h]) load_psi<3>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
+        }
         const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
-        if (mine) {
+        if (mine && PASS == EFM_REV) {
+            // reverse rebuild (-dt, no CPML) into the ping-pong partner f.vo: CPML slabs -> 0,
+            // boundary strips -> the values saved at forward step nt-2-it (:1955-1960),
+            // box interior -> stencil update, never-updated cells -> 0
+            const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!colgrid[h]) continue;
+                const int z = T.z0 + lr + 4 * h;
+                const int hi = hidx[h], ci = cidx[h];
+                const int64_t c = x + SZ * z + SY * y;
+                float nvx = 0.f, nvy = 0.f, nvz = 0.f;
+                const bool zone = x < W || x >= nx - W || y < W || y >= ny - W || z >= nz - W;
+                int64_t slot[3];
+                const int nslot = zone ? 0 : efm_strip_slots(I, x, y, z, slot);
+                if (nslot > 0) {
+                    const float *sv = I.border + (int64_t)(I.nt - 2 - it) * 3 * I.strip_n;
+                    nvx = sv[slot[0]];
+                    nvy = sv[I.strip_n + slot[0]];
+                    nvz = sv[2 * I.strip_n + slot[0]];
+                } else if (!zone && plane_in && colin[h]) {
+                    const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
+                    const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
+                    const float dtxx_dx = t0[hi + 1] - t0[hi];
+                    const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
+                    const float dtyy_dy = R.center(sp, 0)[ci] - R.center(s0, 0)[ci];
+                    const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
+                    const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
+                    const float dtxy_dx = txyc - t3[hi - 1];
+                    const float dtxz_dz = txzc - t4[hi - EFM_HX];
+                    const float dtxz_dx = txzc - t4[hi - 1];
+                    const float dtyz_dz = tyzc - t5[hi - EFM_HX];
+                    const float dtyz_dy = tyzc - R.halo(sm, 4)[hi];
+                    const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];
+                    const float bj = R.halo(sp, 5)[hi];
+                    const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
+                    const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
+                    const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
+                    const float k = I.k;
+                    nvx = R.center(s0, 1)[ci] + k * b_x * (dtxx_dx + dtxy_dy + dtxz_dz);
+                    nvy = R.center(s0, 2)[ci] + k * b_y * (dtxy_dx + dtyy_dy + dtyz_dz);
+                    nvz = R.center(s0, 3)[ci] + k * b_z * (dtxz_dx + dtyz_dy + dtzz_dz);
+                }
+                I.f.vo[0][c] = nvx;
+                I.f.vo[1][c] = nvy;
+                I.f.vo[2][c] = nvz;
+            }
+        } else if (mine) {
             const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -509,6 +558,8 @@ __global__ void efm_model_reciprocals(const float *__restrict__ mu, const float 
     }
 }
 
+cudaError_t efm_image_init_attributes();
+
 // ---------------------------------------------------------------------------- launchers
 static const size_t kSmemStress = (size_t)EFM_SR * (4 * EFM_HALO_BYTES + 7 * EFM_CENTER_BYTES);
 static const size_t kSmemVelocity = (size_t)EFM_SR * (6 * EFM_HALO_BYTES + 4 * EFM_CENTER_BYTES);
@@ -524,7 +575,8 @@ extern "C" cudaError_t efm_launch_stream(int pass, int kind, const EfmInst *inst
     } else {
         switch (pass) {
             case EFM_FWD: efm_velocity_stream<EFM_FWD><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
-            default: efm_velocity_stream<EFM_ADJ><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
+            case EFM_ADJ: efm_velocity_stream<EFM_ADJ><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
+            default: efm_velocity_stream<EFM_REV><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
         }
     }
     return cudaGetLastError();
@@ -546,5 +598,6 @@ extern "C" cudaError_t efm_stream_init_attributes() {
     if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_REV>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss))) return e;
     if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
     if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
-    return cudaSuccess;
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_REV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+    return efm_image_init_attributes();
 }

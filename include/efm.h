@@ -193,11 +193,12 @@ EFM_API int efm_status(efm_ctx *ctx, void *stream);
 #define EFM_K_FWD_VELOCITY 1
 #define EFM_K_ADJ_STRESS 2
 #define EFM_K_ADJ_VELOCITY 3
-#define EFM_K_REV_VELOCITY 4   /* reverse rebuild + imaging */
+#define EFM_K_REV_VELOCITY 4   /* reverse rebuild (+ imaging in the one-thread-per-cell kernels) */
 #define EFM_K_REV_STRESS 5
 #define EFM_K_REDUCE 6         /* residual + misfit reduction */
 #define EFM_K_MODEL_AUX 7      /* 1/mu, 1/rho for the plane-streaming kernels (once per call) */
-#define EFM_NKERN 8
+#define EFM_K_IMAGING 8        /* zero-lag imaging (plane-streaming kernels) */
+#define EFM_NKERN 9
 
 /*
  * Record a CUDA event pair around every kernel launch of this context (enable = 1) so that

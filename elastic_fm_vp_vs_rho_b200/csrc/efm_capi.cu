@@ -13,6 +13,7 @@
 #include <cudaTypedefs.h>
 
 #include "efm.h"
+#include "efm_exact.cuh"
 #include "efm_internal.cuh"
 #include "efm_stream.cuh"
 #include "efm_util.cuh"
@@ -26,6 +27,8 @@ extern "C" cudaError_t efm_launch_stream(int pass, int kind, const EfmInst *inst
 extern "C" cudaError_t efm_stream_init_attributes();
 extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int tiles, int it,
                                         cudaStream_t s);
+extern "C" cudaError_t efm_launch_exact(int kind, const EfmExact *t, int n, int tiles, int step,
+                                        int slot, cudaStream_t s);
 extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho, float *rmu,
                                               float *buoy, int64_t n, cudaStream_t s);
 
@@ -63,6 +66,11 @@ struct Inst {
     bool fields_grad = false;
     float *psi = nullptr;
     float *border = nullptr;
+    // exact adjoint: checkpoints of (v, tau, psi), a segment of per-step (v, tau), and the
+    // adjoint memory variables (two sets, read / written alternately)
+    float *ckpt = nullptr, *segbuf = nullptr, *apsi = nullptr;
+    int ck_every = 0, nck = 0;
+    bool ck_saved = false;
     int64_t ncell = 0, strip_n = 0, psx_n = 0, psy_n = 0, psz_n = 0;
     int64_t gather_off = 0, grad_off = 0;
     int tiles_x = 0, tiles_z = 0, tiles_y = 0, tiles = 0, tile_begin = 0;
@@ -134,6 +142,9 @@ struct efm_ctx {
     // plane-streaming kernels
     int opt_stream = 1;
     int opt_ychunk = 0;
+    int opt_ck_every = 50;
+    EfmExact *d_ex = nullptr;  // exact-adjoint tables, two (memory-variable parities) per instance
+    int ex_cap = 0;
     CUtensorMap *d_maps = nullptr;  // EFM_MAPS_PER_INST per instance
     int maps_cap = 0;
     unsigned int *d_err = nullptr;
@@ -277,6 +288,7 @@ int choose_ychunk(const efm_ctx *ctx, int tz = EFM_STZ, int per_sm = 2) {
     return best;
 }
 
+
 int64_t strip_count(const Inst &I) {
     const int64_t bx = I.nx - 2 * I.W, by = I.ny - 2 * I.W, bz = I.nz - I.W - 2;
     return 4 * by * bz + 4 * bz * bx + 4 * by * bx;
@@ -292,6 +304,11 @@ void free_inst(Inst &I) {
     cudaFree(I.fields);
     cudaFree(I.psi);
     cudaFree(I.border);
+    cudaFree(I.ckpt);
+    cudaFree(I.segbuf);
+    cudaFree(I.apsi);
+    I.ckpt = I.segbuf = I.apsi = nullptr;
+    I.ck_every = I.nck = 0;
     I.cpml = nullptr;
     I.rec_mask = nullptr;
     I.rec_lin = I.rec_id = nullptr;
@@ -449,6 +466,242 @@ int check_ready(efm_ctx *ctx) {
     return ensure_layout(ctx);
 }
 
+
+size_t psi_floats(const Inst &I) { return 6 * (size_t)(I.psx_n + I.psy_n + I.psz_n); }
+size_t ckpt_floats(const Inst &I) { return 9 * (size_t)I.ncell + psi_floats(I); }
+
+// Workspace of the exact adjoint (checkpoint interval from the context option).
+int ensure_exact(efm_ctx *ctx) {
+    for (Inst &I : ctx->inst) {
+        const int K = std::max(1, std::min(ctx->opt_ck_every, I.nt));
+        if (I.ckpt != nullptr && I.ck_every == K) continue;
+        cudaFree(I.ckpt);
+        cudaFree(I.segbuf);
+        cudaFree(I.apsi);
+        I.ckpt = I.segbuf = I.apsi = nullptr;
+        I.ck_every = K;
+        I.nck = (I.nt + K - 1) / K;
+        const size_t nck = (size_t)std::max(1, I.nck - 1);
+        if (cudaMalloc(&I.ckpt, nck * ckpt_floats(I) * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&I.segbuf, (size_t)(K + 1) * 9 * I.ncell * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&I.apsi, 2 * psi_floats(I) * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(EFM_ERR_NOMEM, "cannot allocate exact-adjoint checkpoints (interval " +
+                                           std::to_string(K) + ")");
+        }
+    }
+    return EFM_OK;
+}
+
+// Forward tables (slots T_FWD_S, T_FWD_V) and tensor maps; gathers / strips optional.
+int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cudaStream_t s,
+                    bool *stream_kernels) {
+    int rc;
+    const int n = (int)ctx->inst.size();
+    const bool st = stream_ok(ctx);
+    if (st && (rc = get_encoder())) return rc;
+    const int yc = st ? choose_ychunk(ctx) : 0;
+    std::vector<EfmInst> tab(2 * (size_t)n);
+    std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
+    for (int i = 0; i < n; ++i) {
+        Inst &I = ctx->inst[i];
+        EFM_CK(cudaMemsetAsync(I.fields, 0, 9 * I.ncell * sizeof(float), s));
+        if ((rc = zero_psi(I, s))) return rc;
+        EfmInst d = base_table(I);
+        d.nsteps = I.nt;
+        d.err = ctx->d_err;
+        for (int c = 0; c < 3; ++c) d.f.v[c] = d.f.vo[c] = I.va(c);
+        for (int c = 0; c < 6; ++c) d.f.t[c] = I.tt(c);
+        d.gather = gathers ? gathers + I.gather_off : nullptr;
+        d.border = strips ? I.border : nullptr;
+        EfmInst ds = d, dv = d;
+        if (st) {
+            layout_stream(ds, yc);
+            layout_stream(dv, yc);
+            CUtensorMap *m = maps.data() + (size_t)i * EFM_MAPS_PER_INST;
+            const float *sf[11] = {I.va(0), I.va(1), I.va(2), I.aux, I.lam, I.tt(0), I.tt(1),
+                                   I.tt(2), I.tt(3), I.tt(4), I.tt(5)};
+            for (int q = 0; q < 11; ++q)
+                if ((rc = encode_map(m + M_FWD_S + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
+                                     q < 4 ? EFM_HZ : EFM_STZ)))
+                    return rc;
+            const float *vf[10] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
+                                   I.tt(1), I.va(0), I.va(1), I.va(2)};
+            for (int q = 0; q < 10; ++q)
+                if ((rc = encode_map(m + M_FWD_V + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
+                                     q < 6 ? EFM_HZ : EFM_STZ)))
+                    return rc;
+            ds.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_S;
+            dv.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_V;
+        } else {
+            layout_naive(ds);
+            layout_naive(dv);
+        }
+        tab[i] = ds;
+        tab[(size_t)n + i] = dv;
+    }
+    ctx->tiles[T_FWD_S] = finish_table(tab.data(), n);
+    ctx->tiles[T_FWD_V] = finish_table(tab.data() + n, n);
+    if (st)
+        EFM_CK(cudaMemcpyAsync(ctx->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                               cudaMemcpyHostToDevice, s));
+    EFM_CK(cudaMemcpyAsync(ctx->d_tab, tab.data(), tab.size() * sizeof(EfmInst),
+                           cudaMemcpyHostToDevice, s));
+    if (st && recips)
+        for (const Inst &I : ctx->inst)
+            if ((rc = timed_launch(ctx, EFM_K_MODEL_AUX, s, [&] {
+                     return efm_launch_reciprocals(I.mu, I.rho, I.aux, I.aux + I.ncell, I.ncell, s);
+                 })))
+                return rc;
+    *stream_kernels = st;
+    return EFM_OK;
+}
+
+int forward_step(efm_ctx *ctx, bool st, int it, cudaStream_t s) {
+    const int n = (int)ctx->inst.size();
+    const EfmInst *ts = ctx->d_tab, *tv = ctx->d_tab + n;
+    int rc;
+    if ((rc = timed_launch(ctx, EFM_K_FWD_STRESS, s, [&] {
+             return st ? efm_launch_stream(EFM_FWD, 0, ts, n, ctx->tiles[T_FWD_S], it, s)
+                       : efm_launch_stress(EFM_FWD, ts, n, ctx->tiles[T_FWD_S], it, s);
+         })))
+        return rc;
+    return timed_launch(ctx, EFM_K_FWD_VELOCITY, s, [&] {
+        return st ? efm_launch_stream(EFM_FWD, 1, tv, n, ctx->tiles[T_FWD_V], it, s)
+                  : efm_launch_velocity(EFM_FWD, tv, n, ctx->tiles[T_FWD_V], it, s);
+    });
+}
+
+// Exact gradient: segments from last to first; recompute each from its checkpoint, keeping
+// (v, tau) of every step, then run the transposed steps backwards through it.
+int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, bool mt,
+                   cudaStream_t s) {
+    int rc;
+    const int n = (int)ctx->inst.size();
+    const int nt = ctx->inst[0].nt;
+    for (const Inst &I : ctx->inst) {
+        if (!I.ck_saved)
+            return fail(EFM_ERR_STATE, "EFM_GRAD_EXACT needs a preceding efm_forward with EFM_SAVE_CHECKPOINTS");
+        if (I.nt != nt) return fail(EFM_ERR_ARG, "EFM_GRAD_EXACT needs one record length for all instances");
+    }
+    if (ctx->ex_cap < n) {
+        cudaFree(ctx->d_ex);
+        ctx->d_ex = nullptr;
+        ctx->ex_cap = 0;
+        EFM_CK(cudaMalloc(&ctx->d_ex, 2 * (size_t)n * sizeof(EfmExact)));
+        ctx->ex_cap = n;
+    }
+    std::vector<EfmExact> tab(2 * (size_t)n);
+    int tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        Inst &I = ctx->inst[i];
+        EFM_CK(cudaMemsetAsync(I.bv(0), 0, 9 * I.ncell * sizeof(float), s));
+        EFM_CK(cudaMemsetAsync(I.apsi, 0, 2 * psi_floats(I) * sizeof(float), s));
+        EFM_CK(cudaMemsetAsync(grad + I.grad_off, 0, 3 * I.ncell * sizeof(float), s));
+        if (mt) EFM_CK(cudaMemsetAsync(mtg + (size_t)i * EFM_NSRC * 6, 0, EFM_NSRC * 6 * sizeof(double), s));
+        EfmExact e;
+        std::memset(&e, 0, sizeof(e));
+        e.nx = I.nx;
+        e.ny = I.ny;
+        e.nz = I.nz;
+        e.W = I.W;
+        e.tiles_x = (I.nx + EFM_TX - 1) / EFM_TX;
+        e.tiles_z = (I.nz + EFM_TZ - 1) / EFM_TZ;
+        e.tiles_y = (I.ny + EFM_TY - 1) / EFM_TY;
+        e.tile_begin = tiles;
+        tiles += e.tiles_x * e.tiles_z * e.tiles_y;
+        e.nt = I.nt;
+        e.k = I.dt / I.dx;
+        e.lam = I.lam;
+        e.mu = I.mu;
+        e.rho = I.rho;
+        e.cpml = I.cpml;
+        for (int c = 0; c < 3; ++c) e.bv[c] = I.bv(c);
+        for (int c = 0; c < 6; ++c) e.bt[c] = I.bt(c);
+        e.psx_n = I.psx_n;
+        e.psy_n = I.psy_n;
+        e.psz_n = I.psz_n;
+        e.seg = I.segbuf;
+        e.slot_stride = 9 * I.ncell;
+        e.g_lam = grad + I.grad_off;
+        e.g_mu = grad + I.grad_off + I.ncell;
+        e.g_rho = grad + I.grad_off + 2 * I.ncell;
+        e.nsrc = I.nsrc;
+        for (int q = 0; q < EFM_NSRC; ++q) {
+            e.sx[q] = I.src[q][0];
+            e.sy[q] = I.src[q][1];
+            e.sz[q] = I.src[q][2];
+            for (int c = 0; c < 6; ++c) e.mt[q][c] = I.mt[q][c];
+        }
+        e.wav = I.wav;
+        e.mtg = mt ? mtg + (size_t)i * EFM_NSRC * 6 : nullptr;
+        e.nrec = I.nrec;
+        e.rec_lin = I.rec_lin;
+        e.rec_id = I.rec_id;
+        e.res = res + I.gather_off;
+        const size_t P = psi_floats(I);
+        e.pin = I.apsi;
+        e.pout = I.apsi + P;
+        tab[i] = e;
+        e.pin = I.apsi + P;
+        e.pout = I.apsi;
+        tab[(size_t)n + i] = e;
+    }
+    EFM_CK(cudaMemcpyAsync(ctx->d_ex, tab.data(), tab.size() * sizeof(EfmExact),
+                           cudaMemcpyHostToDevice, s));
+    bool st = false;
+    if ((rc = prepare_forward(ctx, nullptr, false, true, s, &st))) return rc;
+    const int K = ctx->inst[0].ck_every;
+    const int nseg = (nt + K - 1) / K;
+    int parity = 0;
+    for (int k = nseg - 1; k >= 0; --k) {
+        const int first = k * K, last = std::min(nt, first + K) - 1;
+        for (Inst &I : ctx->inst) {
+            if (k == 0) {
+                EFM_CK(cudaMemsetAsync(I.fields, 0, 9 * I.ncell * sizeof(float), s));
+                if ((rc = zero_psi(I, s))) return rc;
+            } else {
+                const float *src = I.ckpt + (size_t)(k - 1) * ckpt_floats(I);
+                EFM_CK(cudaMemcpyAsync(I.fields, src, 9 * I.ncell * sizeof(float),
+                                       cudaMemcpyDeviceToDevice, s));
+                EFM_CK(cudaMemcpyAsync(I.psi, src + 9 * I.ncell, psi_floats(I) * sizeof(float),
+                                       cudaMemcpyDeviceToDevice, s));
+            }
+            EFM_CK(cudaMemcpyAsync(I.segbuf, I.fields, 9 * I.ncell * sizeof(float),
+                                   cudaMemcpyDeviceToDevice, s));
+        }
+        for (int it = first; it <= last; ++it) {
+            if ((rc = forward_step(ctx, st, it, s))) return rc;
+            for (Inst &I : ctx->inst)
+                EFM_CK(cudaMemcpyAsync(I.segbuf + (size_t)(it - first + 1) * 9 * I.ncell, I.fields,
+                                       9 * I.ncell * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        }
+        for (int it = last; it >= first; --it) {
+            const EfmExact *t = ctx->d_ex + (size_t)parity * n;
+            const int slot = it - first + 1;
+            if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
+                     return efm_launch_exact(0, t, n, 0, it, slot, s);
+                 })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
+                     return efm_launch_exact(1, t, n, tiles, it, slot, s);
+                 })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
+                     return efm_launch_exact(2, t, n, tiles, it, slot, s);
+                 })))
+                return rc;
+            parity ^= 1;
+        }
+    }
+    for (Inst &I : ctx->inst) {
+        I.ck_saved = false;
+        I.fwd_saved = false;
+    }
+    return EFM_OK;
+}
+
+
 }  // namespace
 
 // ============================================================================ C ABI
@@ -477,6 +730,7 @@ int efm_destroy(efm_ctx *ctx) {
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     cudaFree(ctx->d_maps);
     cudaFree(ctx->d_err);
+    cudaFree(ctx->d_ex);
     cudaFree(ctx->d_tab);
     cudaFree(ctx->d_seg);
     cudaFree(ctx->d_partial);
@@ -631,85 +885,39 @@ int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders) {
     return b;
 }
 
-int efm_forward(efm_ctx *ctx, float *gathers, int save_borders, void *stream) {
+int efm_forward(efm_ctx *ctx, float *gathers, int save, void *stream) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (gathers == nullptr) return fail(EFM_ERR_ARG, "null gathers");
+    const bool strips = (save & EFM_SAVE_STRIPS) != 0, ckpts = (save & EFM_SAVE_CHECKPOINTS) != 0;
     cudaStream_t s = (cudaStream_t)stream;
-    if ((rc = ensure_workspace(ctx, save_borders != 0, save_borders != 0))) return rc;
-    const int n = (int)ctx->inst.size();
-    const bool st = stream_ok(ctx);
-    if (st && (rc = get_encoder())) return rc;
-    const int yc = st ? choose_ychunk(ctx) : 0;
-    std::vector<EfmInst> tab(2 * (size_t)n);
-    std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
+    if ((rc = ensure_workspace(ctx, strips || ckpts, strips))) return rc;
+    if (ckpts && (rc = ensure_exact(ctx))) return rc;
+    bool st = false;
+    if ((rc = prepare_forward(ctx, gathers, strips, true, s, &st))) return rc;
     int maxnt = 0;
-    for (int i = 0; i < n; ++i) {
-        Inst &I = ctx->inst[i];
-        EFM_CK(cudaMemsetAsync(I.fields, 0, 9 * I.ncell * sizeof(float), s));
-        if ((rc = zero_psi(I, s))) return rc;
-        EfmInst d = base_table(I);
-        d.nsteps = I.nt;
-        d.err = ctx->d_err;
-        for (int c = 0; c < 3; ++c) d.f.v[c] = d.f.vo[c] = I.va(c);
-        for (int c = 0; c < 6; ++c) d.f.t[c] = I.tt(c);
-        d.gather = gathers + I.gather_off;
-        d.border = save_borders ? I.border : nullptr;
-        EfmInst ds = d, dv = d;
-        if (st) {
-            layout_stream(ds, yc);
-            layout_stream(dv, yc);
-            CUtensorMap *m = maps.data() + (size_t)i * EFM_MAPS_PER_INST;
-            const float *sf[11] = {I.va(0), I.va(1), I.va(2), I.aux, I.lam, I.tt(0), I.tt(1),
-                                   I.tt(2), I.tt(3), I.tt(4), I.tt(5)};
-            for (int q = 0; q < 11; ++q)
-                if ((rc = encode_map(m + M_FWD_S + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
-                                     q < 4 ? EFM_HZ : EFM_STZ)))
-                    return rc;
-            const float *vf[10] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
-                                   I.tt(1), I.va(0), I.va(1), I.va(2)};
-            for (int q = 0; q < 10; ++q)
-                if ((rc = encode_map(m + M_FWD_V + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
-                                     q < 6 ? EFM_HZ : EFM_STZ)))
-                    return rc;
-            ds.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_S;
-            dv.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_V;
-        } else {
-            layout_naive(ds);
-            layout_naive(dv);
-        }
-        tab[i] = ds;
-        tab[(size_t)n + i] = dv;
+    for (Inst &I : ctx->inst) {
         maxnt = std::max(maxnt, I.nt);
         I.fwd_saved = false;
+        I.ck_saved = false;
     }
-    ctx->tiles[T_FWD_S] = finish_table(tab.data(), n);
-    ctx->tiles[T_FWD_V] = finish_table(tab.data() + n, n);
-    if (st)
-        EFM_CK(cudaMemcpyAsync(ctx->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
-                               cudaMemcpyHostToDevice, s));
-    EFM_CK(cudaMemcpyAsync(ctx->d_tab, tab.data(), tab.size() * sizeof(EfmInst),
-                           cudaMemcpyHostToDevice, s));
-    if (st)
-        for (const Inst &I : ctx->inst)
-            if ((rc = timed_launch(ctx, EFM_K_MODEL_AUX, s, [&] {
-                     return efm_launch_reciprocals(I.mu, I.rho, I.aux, I.aux + I.ncell, I.ncell, s);
-                 })))
-                return rc;
-    const EfmInst *ts = ctx->d_tab, *tv = ctx->d_tab + n;
     for (int it = 0; it < maxnt; ++it) {
-        if ((rc = timed_launch(ctx, EFM_K_FWD_STRESS, s, [&] {
-                 return st ? efm_launch_stream(EFM_FWD, 0, ts, n, ctx->tiles[T_FWD_S], it, s)
-                           : efm_launch_stress(EFM_FWD, ts, n, ctx->tiles[T_FWD_S], it, s);
-             })))
-            return rc;
-        if ((rc = timed_launch(ctx, EFM_K_FWD_VELOCITY, s, [&] {
-                 return st ? efm_launch_stream(EFM_FWD, 1, tv, n, ctx->tiles[T_FWD_V], it, s)
-                           : efm_launch_velocity(EFM_FWD, tv, n, ctx->tiles[T_FWD_V], it, s);
-             })))
-            return rc;
+        if ((rc = forward_step(ctx, st, it, s))) return rc;
+        if (ckpts)
+            for (Inst &I : ctx->inst)
+                if ((it + 1) % I.ck_every == 0 && it + 1 < I.nt) {
+                    // checkpoint k = (it+1)/K holds the state after step it (k >= 1; 0 = zeros)
+                    float *dst = I.ckpt + (size_t)((it + 1) / I.ck_every - 1) * ckpt_floats(I);
+                    EFM_CK(cudaMemcpyAsync(dst, I.fields, 9 * I.ncell * sizeof(float),
+                                           cudaMemcpyDeviceToDevice, s));
+                    EFM_CK(cudaMemcpyAsync(dst + 9 * I.ncell, I.psi, psi_floats(I) * sizeof(float),
+                                           cudaMemcpyDeviceToDevice, s));
+                }
     }
-    for (Inst &I : ctx->inst) I.fwd_saved = save_borders != 0;
+    for (Inst &I : ctx->inst) {
+        I.fwd_saved = strips;
+        I.ck_saved = ckpts;
+    }
     return EFM_OK;
 }
 
@@ -719,6 +927,12 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     if (rc) return rc;
     const bool model = (flags & EFM_GRAD_MODEL) != 0, mt = (flags & EFM_GRAD_MT) != 0;
     if (!model && !mt) return fail(EFM_ERR_ARG, "flags select no gradient");
+    if (flags & EFM_GRAD_EXACT) {
+        if (res == nullptr || grad == nullptr || (mt && mtg == nullptr))
+            return fail(EFM_ERR_ARG, "null buffer");
+        if ((rc = ensure_workspace(ctx, true, false)) || (rc = ensure_exact(ctx))) return rc;
+        return exact_gradient(ctx, res, grad, mtg, mt, (cudaStream_t)stream);
+    }
     if (res == nullptr) return fail(EFM_ERR_ARG, "null residual");
     if (model && grad == nullptr) return fail(EFM_ERR_ARG, "null gradient buffer");
     if (mt && mtg == nullptr) return fail(EFM_ERR_ARG, "null MT gradient buffer");
@@ -727,7 +941,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
         for (const Inst &I : ctx->inst)
             if (!I.fwd_saved)
                 return fail(EFM_ERR_STATE,
-                            "EFM_GRAD_MODEL needs a preceding efm_forward(..., save_borders=1)");
+                            "EFM_GRAD_MODEL needs a preceding efm_forward(..., EFM_SAVE_STRIPS)");
     cudaStream_t s = (cudaStream_t)stream;
     const int n = (int)ctx->inst.size();
     const bool st = stream_ok(ctx);
@@ -905,6 +1119,10 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             if (value < 0 || value > EFM_MAX_YCHUNK)
                 return fail(EFM_ERR_ARG, "ychunk must be in 0..64 (0 = automatic)");
             ctx->opt_ychunk = value;
+            break;
+        case EFM_OPT_CHECKPOINT_EVERY:
+            if (value < 1 || value > 100000) return fail(EFM_ERR_ARG, "checkpoint interval must be >= 1");
+            ctx->opt_ck_every = value;
             break;
         default: return fail(EFM_ERR_ARG, "unknown option");
     }

@@ -17,7 +17,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import EFM_GRAD_MODEL, EFM_GRAD_MT, EFM_GRAD_NT1, EFM_MAX_SRC, check, ptr, stream_ptr
+from ._lib import (EFM_GRAD_EXACT, EFM_GRAD_MODEL, EFM_GRAD_MT, EFM_GRAD_NT1, EFM_MAX_SRC,
+                   EFM_SAVE_CHECKPOINTS, EFM_SAVE_STRIPS, check, ptr, stream_ptr)
 
 
 def _f32(t):
@@ -165,13 +166,16 @@ class ShotBatch:
         return int(self._L.efm_workspace_bytes(self._ctx, 1 if save_borders else 0))
 
     # ------------------------------------------------------------------ compute
-    def forward(self, save_borders=False, out=None, stream=None):
-        """Forward-model every instance; returns the gather buffer (float32, gather layout)."""
+    def forward(self, save_borders=False, checkpoints=False, out=None, stream=None):
+        """Forward-model every instance; returns the gather buffer (float32, gather layout).
+
+        save_borders: keep the boundary strips the reference-mode gradient rebuilds from;
+        checkpoints: keep full-state checkpoints for the exact gradient."""
         import torch
         if out is None:
             out = torch.empty(self.gather_size, dtype=torch.float32, device="cuda")
-        check(self._L.efm_forward(self._ctx, ptr(out), 1 if save_borders else 0,
-                                  stream_ptr(stream)))
+        save = (EFM_SAVE_STRIPS if save_borders else 0) | (EFM_SAVE_CHECKPOINTS if checkpoints else 0)
+        check(self._L.efm_forward(self._ctx, ptr(out), save, stream_ptr(stream)))
         return out
 
     def residual_misfit(self, mod, obs, res=None, stream=None):
@@ -184,13 +188,18 @@ class ShotBatch:
                                           ptr(mis), stream_ptr(stream)))
         return res, mis
 
-    def gradient(self, res, model=True, mt=False, nt_minus_1=False, stream=None):
+    def gradient(self, res, model=True, mt=False, nt_minus_1=False, exact=False, stream=None):
         """Adjoint pass.  Returns (grad buffer or None, mt grads (ninst, 4, 6) float64 or None).
 
+        Default: the reference's imaging gradient (needs forward(save_borders=True)).
+        exact=True: the exact gradient of 0.5*sum(res^2) w.r.t. lambda, mu, rho (and M with
+        mt=True); needs forward(checkpoints=True).
         nt_minus_1: MT-only pass over nt-1 steps (backwardFields_FowardFieldsRemake length)."""
         import torch
+        if exact:
+            model = True
         flags = ((EFM_GRAD_MODEL if model else 0) | (EFM_GRAD_MT if mt else 0)
-                 | (EFM_GRAD_NT1 if nt_minus_1 else 0))
+                 | (EFM_GRAD_NT1 if nt_minus_1 else 0) | (EFM_GRAD_EXACT if exact else 0))
         g = None
         m = None
         if model:

@@ -52,6 +52,14 @@ extern "C" {
 #define EFM_GRAD_MT 2      /* moment-tensor gradient (source-point strain) */
 #define EFM_GRAD_NT1 4     /* with EFM_GRAD_MT alone: run nt-1 adjoint steps, the loop length
                               of backwardFields_FowardFieldsRemake (:1940) */
+#define EFM_GRAD_EXACT 8   /* exact discrete gradient dJ/d(lambda, mu, rho, M) of
+                              J = 0.5 sum (mod - obs)^2 instead of the reference's imaging
+                              gradient; needs efm_forward(..., EFM_SAVE_CHECKPOINTS) */
+
+/* `save` flags of efm_forward(). */
+#define EFM_SAVE_STRIPS 1       /* boundary strips for the reverse-time rebuild (EFM_GRAD_MODEL) */
+#define EFM_SAVE_CHECKPOINTS 2  /* full-state checkpoints every EFM_OPT_CHECKPOINT_EVERY steps
+                                   (EFM_GRAD_EXACT) */
 
 typedef struct efm_ctx efm_ctx;
 
@@ -111,11 +119,11 @@ EFM_API int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders);
 /*
  * Forward modelling of every instance (Elastic3D.forwardFields, :1812-1847 with
  * kernel_Tau :59-128, addSource :1728-1734, kernel_Vx_Vy_Vz :133-188,
- * kernel_get_Station :324-335 and, when save_borders, kernel_get_border :378-419).
- * Fields start from zero.  gathers_dev: efm_gather_size() floats.
- * save_borders = 1 keeps what efm_gradient(EFM_GRAD_MODEL) needs.
+ * kernel_get_Station :324-335 and, with EFM_SAVE_STRIPS, kernel_get_border :378-419).
+ * Fields start from zero.  gathers_dev: efm_gather_size() floats.  `save`: EFM_SAVE_*
+ * flags -- what the following efm_gradient needs.
  */
-EFM_API int efm_forward(efm_ctx *ctx, float *gathers_dev, int save_borders, void *stream);
+EFM_API int efm_forward(efm_ctx *ctx, float *gathers_dev, int save, void *stream);
 
 /*
  * Adjoint pass (Elastic3D.backwardFields_FowardFieldsRemake, :1929-2054, and
@@ -178,6 +186,9 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 /* Planes per block of the plane-streaming kernels; 0 (default) picks the chunk that fills
  * whole waves of blocks best. */
 #define EFM_OPT_YCHUNK 2
+/* Steps between full-state checkpoints of EFM_SAVE_CHECKPOINTS (default 50); memory per
+ * instance ~ (nt/K) checkpoints + (K+1) stored steps of the 9 fields. */
+#define EFM_OPT_CHECKPOINT_EVERY 3
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*

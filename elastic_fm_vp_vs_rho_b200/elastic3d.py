@@ -15,8 +15,10 @@ Differences that are deliberate (documented per method):
 * no module globals: the reference's classes read ``nx, ny, nz, fq, nSismos, rank,
   sizeRank, SrcIdx`` from ``__main__``; here they are attributes of the objects;
 * ``Wavelet`` takes an optional ``dt`` (the reference hard-codes 0.0855198 s, :1254);
-* all earthquakes of ``fwi_Vp_Vs_Rho`` / ``fwi_Mij`` run as one batch on the GPU instead of
-  one MPI rank per GPU; multi-GPU sharding is :mod:`elastic_fm_vp_vs_rho_b200.distributed`;
+* all earthquakes of ``fwi_Vp_Vs_Rho`` run as one batch on the GPU instead of one MPI rank
+  per earthquake; under torch.distributed each rank batches a contiguous shard and one
+  all-reduce per evaluation sums gradients and misfits
+  (:mod:`elastic_fm_vp_vs_rho_b200.distributed`);
 * plots are not drawn; result files are written only when ``results_dir`` is set.
 
 Host arrays (``Model.Vp`` ...) are numpy float32 ``(ny, nz, nx)`` as in the reference;
@@ -31,6 +33,7 @@ import os
 import numpy as np
 
 from . import _lib, configs
+from . import distributed as _dist
 from .engine import ShotBatch, smooth_mask
 from . import lbfgs as _lbfgs
 
@@ -533,24 +536,35 @@ class Elastic3D:
 
     # ---------------------------------------------------------------- Vp/Vs/Rho FWI
     def _all_shots_engine(self, listaTM):
+        """This rank's earthquakes (all of them without torch.distributed) as one batch."""
+        lo, hi = _dist.shard(self.geometria.getLenSismos())
         eng = ShotBatch()
-        for k in range(self.geometria.getLenSismos()):
+        for k in range(lo, hi):
             eng.add(**self._instance_kwargs(k, listaTM[k].as_array()))
+        self._shard = (lo, hi)
         return eng
 
     def _shots_misfit(self, eng, obs_flat, want_grad):
         """Forward all shots; optionally the summed lambda/mu/rho gradient."""
         torch = _torch()
-        mod = eng.forward(save_borders=want_grad)
-        res, mis = eng.residual_misfit(mod, obs_flat)
-        total = float(mis.sum().item())
-        if not want_grad:
-            return total, None
-        g, _ = eng.gradient(res, model=True)
-        acc = torch.zeros((3, self.ny, self.nz, self.nx), dtype=torch.float32, device="cuda")
-        for i in range(len(eng)):
-            acc += eng.grad_view(g, i)
-        return total, acc
+        if len(eng) == 0:  # a rank without shots still joins the collectives
+            acc = torch.zeros((3, self.ny, self.nz, self.nx), dtype=torch.float32, device="cuda")
+            tot = torch.zeros(1, dtype=torch.float64, device="cuda")
+        else:
+            mod = eng.forward(save_borders=want_grad)
+            res, mis = eng.residual_misfit(mod, obs_flat)
+            tot = mis.sum().reshape(1)
+            acc = torch.zeros((3, self.ny, self.nz, self.nx), dtype=torch.float32, device="cuda")
+            if want_grad:
+                g, _ = eng.gradient(res, model=True)
+                for i in range(len(eng)):
+                    acc += eng.grad_view(g, i)
+        # one collective per call: gradients (when wanted) + misfit summed over ranks
+        if want_grad:
+            acc, tot = _dist.all_reduce_sum(acc, tot)
+            return float(tot.item()), acc
+        (tot,) = _dist.all_reduce_sum(tot)
+        return float(tot.item()), None
 
     def _update_vp_vs_rho(self, cRho_top):
         """compute_Vp_Vs with the current rho, compute_Rho, keep rho's top 10 planes
@@ -584,9 +598,11 @@ class Elastic3D:
         L = int(lbfgsLayers)
         skL = torch.zeros((L,) + shape, dtype=torch.float32, device="cuda")
         ykL, skM, ykM, skR, ykR = (torch.zeros_like(skL) for _ in range(5))
-        obs_flat = torch.cat([torch.as_tensor(np.stack([d.Vx, d.Vy, d.Vz]).astype(np.float32))
-                              .reshape(-1) for d in data_obs]).cuda()
         eng = self._all_shots_engine(listaTM)
+        lo, hi = self._shard
+        obs_flat = torch.cat([torch.as_tensor(np.stack([d.Vx, d.Vy, d.Vz]).astype(np.float32))
+                              .reshape(-1) for d in data_obs[lo:hi]]
+                             + [torch.zeros(0)]).cuda()
         tmp = torch.empty(shape, dtype=torch.float32, device="cuda")
         nTry = 10
         self.fwi_gradients = None

@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--grid", default="128,128,96", help="nx,ny,nz")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-tune", action="store_true",
+                   help="skip the launch-shape autotuner (default tile rows / y-chunk)")
     p.add_argument("--traffic-file", default=os.path.join(REPO, "profiles", "ncu_traffic.json"))
     return p.parse_args()
 
@@ -288,6 +290,10 @@ def main():
     d_vp, d_vs = dev(w.vp0), dev(w.vs0)
     eng = ShotBatch()
     eng.add(lam=d_lam, mu=d_mu, rho=d_rho, **kw)
+    tuned = None
+    if not args.no_tune:
+        from elastic_fm_vp_vs_rho_b200 import autotune
+        tuned = autotune.tune(eng, use_cache=False)
     L = _lib.load()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     red = torch.zeros(3 * w.ncells + 1, dtype=torch.float32, device="cuda")
@@ -310,8 +316,6 @@ def main():
     if world > 1:
         dist.barrier()
     check = lambda rc: _lib.check(rc)  # noqa: E731
-    check(L.efm_kernel_stats(eng._ctx, None, None, 1))
-    check(L.efm_set_timing(eng._ctx, 1))
     sampler = ClockSampler(local)
     sampler.start()
     times = []
@@ -326,6 +330,16 @@ def main():
         times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     clocks = sampler.stop()
+    eng.status()
+    # per-kernel device times: the same steps again with an event pair around every launch
+    # (outside the timed region, which runs without them)
+    stat_steps = min(args.steps, 3)
+    check(L.efm_kernel_stats(eng._ctx, None, None, 1))
+    check(L.efm_set_timing(eng._ctx, 1))
+    for _ in range(stat_steps):
+        flush.fill_(1.0)
+        step()
+    torch.cuda.synchronize()
     check(L.efm_set_timing(eng._ctx, 0))
     launches = (__import__("ctypes").c_int64 * _lib.EFM_NKERN)()
     kms = (__import__("ctypes").c_double * _lib.EFM_NKERN)()
@@ -338,8 +352,9 @@ def main():
         dist.barrier()
     upd = cell_updates(w)
     value = world * upd * args.steps / (total_ms * 1e-3) / 1e9
-    # the misfit reduction is two kernels per call; the chain rule one kernel per step
-    gpu_launches = int(sum(launches)) + int(launches[6]) + args.steps
+    # launches per step from the statistics pass (the misfit reduction is two kernels per
+    # call; the chain rule one kernel per step), times the timed steps
+    gpu_launches = (int(sum(launches)) + int(launches[6]) + stat_steps) * args.steps // stat_steps
 
     # roofline of the dominant kernel
     alg = algorithmic_bytes(w)
@@ -385,7 +400,10 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded layered + anomaly model, MT source)",
-                "config": config_dict(w, args, world), "gpu_launches": gpu_launches,
+                "config": dict(config_dict(w, args, world), launch_shape=tuned and {
+                    "tile_rows": tuned["rows"], "ychunk": tuned["ychunk"],
+                    "source": "autotuned (probe of %d steps)" % tuned["nt_probe"]}),
+                "gpu_launches": gpu_launches,
                 "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
         print(json.dumps(line), flush=True)
     eng.close()

@@ -22,8 +22,8 @@ extern "C" cudaError_t efm_launch_stress(int pass, const EfmInst *insts, int nin
                                          int it, cudaStream_t s);
 extern "C" cudaError_t efm_launch_velocity(int pass, const EfmInst *insts, int ninst, int tiles,
                                            int it, cudaStream_t s);
-extern "C" cudaError_t efm_launch_stream(int pass, int kind, const EfmInst *insts, int ninst,
-                                         int tiles, int it, cudaStream_t s);
+extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, const EfmInst *insts,
+                                         int ninst, int tiles, int it, cudaStream_t s);
 extern "C" cudaError_t efm_stream_init_attributes();
 extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int tiles, int it,
                                         cudaStream_t s);
@@ -142,6 +142,8 @@ struct efm_ctx {
     // plane-streaming kernels
     int opt_stream = 1;
     int opt_ychunk = 0;
+    int opt_rows = 0;
+    int rows = 2;  // cells per thread of the tables last built for the streaming kernels
     int opt_ck_every = 50;
     EfmExact *d_ex = nullptr;  // exact-adjoint tables, two (memory-variable parities) per instance
     int ex_cap = 0;
@@ -244,7 +246,7 @@ void layout_naive(EfmInst &d) {
     d.ychunk = 0;
 }
 
-void layout_stream(EfmInst &d, int ychunk, int tz = EFM_STZ) {
+void layout_stream(EfmInst &d, int ychunk, int tz) {
     d.tiles_x = (d.nx + EFM_STX - 1) / EFM_STX;
     d.tiles_z = (d.nz + tz - 1) / tz;
     d.ychunk = ychunk;
@@ -263,7 +265,7 @@ int finish_table(EfmInst *t, int n) {
 
 // Planes per streaming block: the chunk that fills whole waves of blocks best, for tiles of
 // EFM_STX x tz cells and `per_sm` resident blocks per SM.
-int choose_ychunk(const efm_ctx *ctx, int tz = EFM_STZ, int per_sm = 2) {
+int choose_ychunk(const efm_ctx *ctx, int tz, int per_sm) {
     if (ctx->opt_ychunk > 0) return ctx->opt_ychunk;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
@@ -500,7 +502,9 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
     const int n = (int)ctx->inst.size();
     const bool st = stream_ok(ctx);
     if (st && (rc = get_encoder())) return rc;
-    const int yc = st ? choose_ychunk(ctx) : 0;
+    const int rows = ctx->rows = ctx->opt_rows == 1 ? 1 : 2;
+    const int tz = efm_st_tz(rows), hz = efm_st_hz(rows);
+    const int yc = st ? choose_ychunk(ctx, tz, rows == 1 ? 3 : 2) : 0;
     std::vector<EfmInst> tab(2 * (size_t)n);
     std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
     for (int i = 0; i < n; ++i) {
@@ -516,20 +520,20 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
         d.border = strips ? I.border : nullptr;
         EfmInst ds = d, dv = d;
         if (st) {
-            layout_stream(ds, yc);
-            layout_stream(dv, yc);
+            layout_stream(ds, yc, tz);
+            layout_stream(dv, yc, tz);
             CUtensorMap *m = maps.data() + (size_t)i * EFM_MAPS_PER_INST;
             const float *sf[11] = {I.va(0), I.va(1), I.va(2), I.aux, I.lam, I.tt(0), I.tt(1),
                                    I.tt(2), I.tt(3), I.tt(4), I.tt(5)};
             for (int q = 0; q < 11; ++q)
                 if ((rc = encode_map(m + M_FWD_S + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
-                                     q < 4 ? EFM_HZ : EFM_STZ)))
+                                     q < 4 ? hz : tz)))
                     return rc;
             const float *vf[10] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
                                    I.tt(1), I.va(0), I.va(1), I.va(2)};
             for (int q = 0; q < 10; ++q)
                 if ((rc = encode_map(m + M_FWD_V + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
-                                     q < 6 ? EFM_HZ : EFM_STZ)))
+                                     q < 6 ? hz : tz)))
                     return rc;
             ds.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_S;
             dv.tmap = ctx->d_maps + (size_t)i * EFM_MAPS_PER_INST + M_FWD_V;
@@ -562,12 +566,12 @@ int forward_step(efm_ctx *ctx, bool st, int it, cudaStream_t s) {
     const EfmInst *ts = ctx->d_tab, *tv = ctx->d_tab + n;
     int rc;
     if ((rc = timed_launch(ctx, EFM_K_FWD_STRESS, s, [&] {
-             return st ? efm_launch_stream(EFM_FWD, 0, ts, n, ctx->tiles[T_FWD_S], it, s)
+             return st ? efm_launch_stream(EFM_FWD, 0, ctx->rows, ts, n, ctx->tiles[T_FWD_S], it, s)
                        : efm_launch_stress(EFM_FWD, ts, n, ctx->tiles[T_FWD_S], it, s);
          })))
         return rc;
     return timed_launch(ctx, EFM_K_FWD_VELOCITY, s, [&] {
-        return st ? efm_launch_stream(EFM_FWD, 1, tv, n, ctx->tiles[T_FWD_V], it, s)
+        return st ? efm_launch_stream(EFM_FWD, 1, ctx->rows, tv, n, ctx->tiles[T_FWD_V], it, s)
                   : efm_launch_velocity(EFM_FWD, tv, n, ctx->tiles[T_FWD_V], it, s);
     });
 }
@@ -824,11 +828,11 @@ int efm_add_instance(efm_ctx *ctx, const efm_instance_desc *d, int *id) {
     if ((e = cudaMemcpy(I.rec_lin, lin.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
     if ((e = cudaMemcpy(I.rec_id, rid.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
     {
-        const int tx = (I.nx + EFM_STX - 1) / EFM_STX, tz = (I.nz + EFM_STZ - 1) / EFM_STZ;
+        const int tx = (I.nx + EFM_STX - 1) / EFM_STX, tz = (I.nz + EFM_REC_TZ - 1) / EFM_REC_TZ;
         std::vector<uint8_t> rt((size_t)I.ny * tz * tx, 0);
         for (int r = 0; r < I.nrec; ++r) {
             const int x = I.rec[3 * r], y = I.rec[3 * r + 1], z = I.rec[3 * r + 2];
-            rt[((size_t)y * tz + z / EFM_STZ) * tx + x / EFM_STX] = 1;
+            rt[((size_t)y * tz + z / EFM_REC_TZ) * tx + x / EFM_STX] = 1;
         }
         if ((e = cudaMalloc(&I.rec_tile, rt.size()))) return bad(e);
         if ((e = cudaMemcpy(I.rec_tile, rt.data(), rt.size(), cudaMemcpyHostToDevice))) return bad(e);
@@ -946,7 +950,9 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     const int n = (int)ctx->inst.size();
     const bool st = stream_ok(ctx);
     if (st && (rc = get_encoder())) return rc;
-    const int yc = st ? choose_ychunk(ctx) : 0;
+    const int rows = ctx->rows = ctx->opt_rows == 1 ? 1 : 2;
+    const int tz = efm_st_tz(rows), hz = efm_st_hz(rows);
+    const int yc = st ? choose_ychunk(ctx, tz, rows == 1 ? 3 : 2) : 0;
     const int yci = st ? choose_ychunk(ctx, EFM_IMG_TZ, 3) : 0;
     std::vector<EfmInst> tab((size_t)T_NSLOT * n);
     std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
@@ -972,19 +978,19 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
         a.mtg = mt ? mtg + (size_t)i * EFM_NSRC * 6 : nullptr;
         EfmInst as = a, av = a;
         if (st) {
-            layout_stream(as, yc);
-            layout_stream(av, yc);
+            layout_stream(as, yc, tz);
+            layout_stream(av, yc, tz);
             const float *sf[11] = {I.bv(0), I.bv(1), I.bv(2), I.aux, I.lam, I.bt(0), I.bt(1),
                                    I.bt(2), I.bt(3), I.bt(4), I.bt(5)};
             for (int q = 0; q < 11; ++q)
                 if ((rc = encode_map(m + M_ADJ_S + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
-                                     q < 4 ? EFM_HZ : EFM_STZ)))
+                                     q < 4 ? hz : tz)))
                     return rc;
             const float *vf[10] = {I.bt(0), I.bt(2), I.bt(3), I.bt(4), I.bt(5), I.aux + I.ncell,
                                    I.bt(1), I.bv(0), I.bv(1), I.bv(2)};
             for (int q = 0; q < 10; ++q)
                 if ((rc = encode_map(m + M_ADJ_V + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
-                                     q < 6 ? EFM_HZ : EFM_STZ)))
+                                     q < 6 ? hz : tz)))
                     return rc;
             as.tmap = dm + M_ADJ_S;
             av.tmap = dm + M_ADJ_V;
@@ -1017,23 +1023,23 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
             }
             EfmInst rv = r, rs = r, ri = r;
             if (st) {
-                layout_stream(rs, yc);
+                layout_stream(rs, yc, tz);
                 const int mb = p == 0 ? M_REV_S0 : M_REV_S1;
                 const float *sf[11] = {r.f.vo[0], r.f.vo[1], r.f.vo[2], I.aux, I.lam, I.tt(0),
                                        I.tt(1), I.tt(2), I.tt(3), I.tt(4), I.tt(5)};
                 for (int q = 0; q < 11; ++q)
                     if ((rc = encode_map(m + mb + q, sf[q], I, q < 4 ? EFM_HX : EFM_STX,
-                                         q < 4 ? EFM_HZ : EFM_STZ)))
+                                         q < 4 ? hz : tz)))
                         return rc;
                 rs.tmap = dm + mb;
                 // reverse velocity rebuild: the velocity pass's fields, old velocity in f.v
-                layout_stream(rv, yc);
+                layout_stream(rv, yc, tz);
                 const int mv = p == 0 ? M_REV_V0 : M_REV_V1;
                 const float *vf[10] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
                                        I.tt(1), r.f.v[0], r.f.v[1], r.f.v[2]};
                 for (int q = 0; q < 10; ++q)
                     if ((rc = encode_map(m + mv + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
-                                         q < 6 ? EFM_HZ : EFM_STZ)))
+                                         q < 6 ? hz : tz)))
                         return rc;
                 rv.tmap = dm + mv;
                 // imaging: halo fV_present + 1/mu (72 x 7 from z0-2), cells 64 x 4
@@ -1077,12 +1083,12 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     auto dtab = [&](int k) { return (const EfmInst *)(ctx->d_tab + (size_t)k * n); };
     for (int it = 0; it < maxsteps; ++it) {
         if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
-                 return st ? efm_launch_stream(EFM_ADJ, 0, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
+                 return st ? efm_launch_stream(EFM_ADJ, 0, ctx->rows, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
                            : efm_launch_stress(EFM_ADJ, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s);
              })))
             return rc;
         if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
-                 return st ? efm_launch_stream(EFM_ADJ, 1, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s)
+                 return st ? efm_launch_stream(EFM_ADJ, 1, ctx->rows, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s)
                            : efm_launch_velocity(EFM_ADJ, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s);
              })))
             return rc;
@@ -1091,7 +1097,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
             const int ki = (it & 1) ? T_IMG1 : T_IMG0;
             // stream kernels: rebuild, then imaging; otherwise one fused rebuild + imaging kernel
             if ((rc = timed_launch(ctx, EFM_K_REV_VELOCITY, s, [&] {
-                     return st ? efm_launch_stream(EFM_REV, 1, dtab(kv), n, ctx->tiles[kv], it, s)
+                     return st ? efm_launch_stream(EFM_REV, 1, ctx->rows, dtab(kv), n, ctx->tiles[kv], it, s)
                                : efm_launch_velocity(EFM_REV, dtab(kv), n, ctx->tiles[kv], it, s);
                  })))
                 return rc;
@@ -1100,7 +1106,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                        })))
                 return rc;
             if ((rc = timed_launch(ctx, EFM_K_REV_STRESS, s, [&] {
-                     return st ? efm_launch_stream(EFM_REV, 0, dtab(ks), n, ctx->tiles[ks], it, s)
+                     return st ? efm_launch_stream(EFM_REV, 0, ctx->rows, dtab(ks), n, ctx->tiles[ks], it, s)
                                : efm_launch_stress(EFM_REV, dtab(ks), n, ctx->tiles[ks], it, s);
                  })))
                 return rc;
@@ -1123,6 +1129,10 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
         case EFM_OPT_CHECKPOINT_EVERY:
             if (value < 1 || value > 100000) return fail(EFM_ERR_ARG, "checkpoint interval must be >= 1");
             ctx->opt_ck_every = value;
+            break;
+        case EFM_OPT_TILE_ROWS:
+            if (value < 0 || value > 2) return fail(EFM_ERR_ARG, "tile rows must be 0, 1 or 2");
+            ctx->opt_rows = value;
             break;
         default: return fail(EFM_ERR_ARG, "unknown option");
     }

@@ -1,12 +1,12 @@
 // Plane-streaming stress / velocity kernels: TMA-fed shared-memory rings.
 //
-// Each block owns a 64 x 8 (x, z) column of the grid and marches along y over a chunk of
-// planes.  One thread issues, per plane, a TMA tile load of every field the half-step reads
-// into one stage of a 4-deep ring (x/z-neighbour fields with a halo box 72 x 10 starting at
-// (x0-4, z0-1); cell-only fields with a 64 x 8 box).  While the block computes plane j from
-// the stages of planes j-1, j, j+1, plane j+2 is in flight; two blocks per SM keep ~100 KB
-// in flight without spending registers.  Each thread computes the cells (x, z) and
-// (x, z+4) of every plane.
+// Each block owns a 64 x TZ (x, z) column of the grid (TZ = 4 * ROWS) and marches along y
+// over a chunk of planes.  One thread issues, per plane, a TMA tile load of every field the
+// half-step reads into one stage of a 4-deep ring (x/z-neighbour fields with a halo box
+// 72 x (TZ + 2) starting at (x0-4, z0-1); cell-only fields with a 64 x TZ box).  While the
+// block computes plane j from the stages of planes j-1, j, j+1, plane j+2 is in flight, so
+// the resident blocks keep ~100 KB per SM in flight without spending registers.  Each
+// thread computes the cells (x, z0 + r + 4h), h < ROWS, of every plane.
 //
 // Per plane the compute touches no global memory it has to wait for except the compact
 // CPML memory variables of PML cells, which are requested before the stage wait.  Sources
@@ -29,7 +29,9 @@ __device__ __forceinline__ float frcp(float a) {
     return r;
 }
 
+template <int ROWS>
 struct Ring {
+    static constexpr int HB = efm_halo_bytes(ROWS), CB = efm_center_bytes(ROWS);
     unsigned char *base;
     uint64_t *bar;
     int stage_bytes;
@@ -38,33 +40,34 @@ struct Ring {
     __device__ __forceinline__ int stage(int p) const { return (p - p0) & (EFM_SR - 1); }
     __device__ __forceinline__ uint32_t parity(int p) const { return ((p - p0) / EFM_SR) & 1; }
     __device__ __forceinline__ const float *halo(int s, int f) const {
-        return reinterpret_cast<const float *>(base + s * stage_bytes + f * EFM_HALO_BYTES);
+        return reinterpret_cast<const float *>(base + s * stage_bytes + f * HB);
     }
     __device__ __forceinline__ const float *center(int s, int f) const {
-        return reinterpret_cast<const float *>(base + s * stage_bytes + nh * EFM_HALO_BYTES +
-                                               f * EFM_CENTER_BYTES);
+        return reinterpret_cast<const float *>(base + s * stage_bytes + nh * HB + f * CB);
     }
 };
 
-template <int NH, int NC>
-__device__ __forceinline__ void issue_plane(const Ring &R, const CUtensorMap *tm, int x0, int z0,
-                                            int p) {
+template <int ROWS, int NH, int NC>
+__device__ __forceinline__ void issue_plane(const Ring<ROWS> &R, const CUtensorMap *tm, int x0,
+                                            int z0, int p) {
+    constexpr int HB = efm_halo_bytes(ROWS), CB = efm_center_bytes(ROWS);
     const int s = R.stage(p);
     uint64_t *bar = &R.bar[s];
     unsigned char *st = R.base + s * R.stage_bytes;
-    efm_mbar_expect_tx(bar, NH * EFM_HALO_TX + NC * EFM_CENTER_TX);
+    efm_mbar_expect_tx(bar, NH * efm_halo_tx(ROWS) + NC * CB);
 #pragma unroll
     for (int f = 0; f < NH; ++f)
-        efm_tma_load_3d(st + f * EFM_HALO_BYTES, tm + f, bar, x0 - EFM_HX_OFF, z0 - 1, p);
+        efm_tma_load_3d(st + f * HB, tm + f, bar, x0 - EFM_HX_OFF, z0 - 1, p);
 #pragma unroll
     for (int f = 0; f < NC; ++f)
-        efm_tma_load_3d(st + NH * EFM_HALO_BYTES + f * EFM_CENTER_BYTES, tm + NH + f, bar, x0, z0, p);
+        efm_tma_load_3d(st + NH * HB + f * CB, tm + NH + f, bar, x0, z0, p);
 }
 
 struct Tile {
     int tx, tz, x0, z0, ys, ye;
 };
 
+template <int ROWS>
 __device__ __forceinline__ Tile stream_tile(const EfmInst &I, int block) {
     const int lt = block - I.tile_begin;
     Tile t;
@@ -73,19 +76,20 @@ __device__ __forceinline__ Tile stream_tile(const EfmInst &I, int block) {
     t.tz = rem % I.tiles_z;
     const int ty = rem / I.tiles_z;
     t.x0 = t.tx * EFM_STX;
-    t.z0 = t.tz * EFM_STZ;
+    t.z0 = t.tz * efm_st_tz(ROWS);
     t.ys = ty * I.ychunk;
     t.ye = min(I.ny, t.ys + I.ychunk);
     return t;
 }
 
-__device__ void drain(const Ring &R, int first, int last) {
+template <int ROWS>
+__device__ void drain(const Ring<ROWS> &R, int first, int last) {
     for (int p = first; p <= last; ++p) efm_mbar_wait(&R.bar[R.stage(p)], R.parity(p), nullptr);
 }
 
 // Block set-up shared by both kernels: barriers, prologue loads, source flag, receiver bits.
-template <int NH, int NC>
-__device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ring &R,
+template <int ROWS, int NH, int NC>
+__device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ring<ROWS> &R,
                                              const CUtensorMap *tm, int *s_flags,
                                              unsigned long long *s_recbits) {
     if (threadIdx.x == 0) {
@@ -94,17 +98,24 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
         int f = 0;
         for (int s = 0; s < I.nsrc; ++s)
             if (I.sx[s] >= T.x0 && I.sx[s] < T.x0 + EFM_STX && I.sz[s] >= T.z0 &&
-                I.sz[s] < T.z0 + EFM_STZ && I.sy[s] >= T.ys && I.sy[s] < T.ye)
+                I.sz[s] < T.z0 + efm_st_tz(ROWS) && I.sy[s] >= T.ys && I.sy[s] < T.ye)
                 f = 1;
         *s_flags = f;
     }
     if (threadIdx.x < 32) {
-        // bit q: plane ys + q holds a receiver inside this tile
+        // bit q: plane ys + q holds a receiver inside this tile (map rows are EFM_REC_TZ high)
         const int l = threadIdx.x;
-        const int64_t row = (int64_t)I.tiles_z * I.tiles_x;
-        const int64_t off = (int64_t)T.tz * I.tiles_x + T.tx;
-        const bool a = T.ys + l < T.ye && I.rec_tile[(int64_t)(T.ys + l) * row + off];
-        const bool b = T.ys + 32 + l < T.ye && I.rec_tile[(int64_t)(T.ys + 32 + l) * row + off];
+        const int nz4 = (I.nz + EFM_REC_TZ - 1) / EFM_REC_TZ;
+        const int64_t row = (int64_t)nz4 * I.tiles_x;
+        bool a = false, b = false;
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            const int z4 = T.tz * ROWS + r;
+            if (z4 >= nz4) break;
+            const int64_t off = (int64_t)z4 * I.tiles_x + T.tx;
+            a = a || (T.ys + l < T.ye && I.rec_tile[(int64_t)(T.ys + l) * row + off]);
+            b = b || (T.ys + 32 + l < T.ye && I.rec_tile[(int64_t)(T.ys + 32 + l) * row + off]);
+        }
         const unsigned lo = __ballot_sync(0xffffffffu, a), hi = __ballot_sync(0xffffffffu, b);
         if (l == 0) *s_recbits = (unsigned long long)lo | ((unsigned long long)hi << 32);
     }
@@ -112,13 +123,13 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
     if (threadIdx.x == 0) {
         for (int q = 0; q < NH + NC; ++q) efm_prefetch_tmap(tm + q);
         for (int p = R.p0; p <= min(T.ye, R.p0 + EFM_SR - 1); ++p)
-            issue_plane<NH, NC>(R, tm, T.x0, T.z0, p);
+            issue_plane<ROWS, NH, NC>(R, tm, T.x0, T.z0, p);
     }
 }
 
 // ------------------------------------------------------------------------------ stress
-template <int PASS>
-__device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring &R, int sm, int s0,
+template <int PASS, int ROWS>
+__device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS> &R, int sm, int s0,
                                             int sp, int it, int x, int y, int z, int hidx,
                                             int cidx, bool has_src, const float *pp) {
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
@@ -267,8 +278,8 @@ __device__ __forceinline__ void load_psi(const EfmInst &I, int x, int y, int z, 
 }  // namespace
 
 // halo fields: vx vy vz 1/mu ; center fields: lambda txx tyy tzz txy txz tyz
-template <int PASS>
-__global__ void __launch_bounds__(EFM_STHREADS, 2)
+template <int PASS, int ROWS>
+__global__ void __launch_bounds__(EFM_STHREADS, ROWS == 1 ? 3 : 2)
 efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     constexpr int NH = 4, NC = 7;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -277,18 +288,18 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     __shared__ unsigned long long s_rec;
     const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
     if (it >= I.nsteps) return;
-    const Tile T = stream_tile(I, blockIdx.x);
+    const Tile T = stream_tile<ROWS>(I, blockIdx.x);
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
-    Ring R{smem, bars, NH * EFM_HALO_BYTES + NC * EFM_CENTER_BYTES, NH, T.ys - 1};
-    stream_setup<NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    Ring<ROWS> R{smem, bars, NH * Ring<ROWS>::HB + NC * Ring<ROWS>::CB, NH, T.ys - 1};
+    stream_setup<ROWS, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const bool has_src = s_src != 0;
-    bool colin[2];
-    int hidx[2], cidx[2];
+    bool colin[ROWS];
+    int hidx[ROWS], cidx[ROWS];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < ROWS; ++h) {
         const int lz = lr + 4 * h, z = T.z0 + lz;
         hidx[h] = (lz + 1) * EFM_HX + lx + EFM_HX_OFF;
         cidx[h] = lz * EFM_STX + lx;
@@ -305,25 +316,25 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     }
     for (int j = T.ys; j < T.ye && ok; ++j) {
         const bool plane_in = j >= EFM_HS && j < ny - EFM_HS && !(PASS == EFM_REV && (j < W || j >= ny - W));
-        float pp[2][9];
+        float pp[ROWS][9];
         if (PASS != EFM_REV) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
+            for (int h = 0; h < ROWS; ++h)
                 if (plane_in && colin[h]) load_psi<0>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
         }
         const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
         if (mine && plane_in) {
             const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
+            for (int h = 0; h < ROWS; ++h)
                 if (colin[h])
-                    stress_cell<PASS>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, hidx[h],
+                    stress_cell<PASS, ROWS>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, hidx[h],
                                       cidx[h], has_src, pp[h]);
         }
         ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
         if (!ok) break;
         if (j - 1 + EFM_SR <= last) {
-            if (threadIdx.x == 0) issue_plane<NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
+            if (threadIdx.x == 0) issue_plane<ROWS, NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
             issued_hi = j - 1 + EFM_SR;
         }
     }
@@ -331,8 +342,8 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
 }
 
 // halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint)
-template <int PASS>
-__global__ void __launch_bounds__(EFM_STHREADS, 2)
+template <int PASS, int ROWS>
+__global__ void __launch_bounds__(EFM_STHREADS, ROWS == 1 ? 3 : 2)
 efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     constexpr int NH = 6, NC = 4;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -341,18 +352,18 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     __shared__ unsigned long long s_rec;
     const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
     if (it >= I.nsteps) return;
-    const Tile T = stream_tile(I, blockIdx.x);
+    const Tile T = stream_tile<ROWS>(I, blockIdx.x);
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
-    Ring R{smem, bars, NH * EFM_HALO_BYTES + NC * EFM_CENTER_BYTES, NH, T.ys - 1};
-    stream_setup<NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    Ring<ROWS> R{smem, bars, NH * Ring<ROWS>::HB + NC * Ring<ROWS>::CB, NH, T.ys - 1};
+    stream_setup<ROWS, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const unsigned long long recbits = s_rec;
-    bool colin[2], colgrid[2];
-    int hidx[2], cidx[2];
+    bool colin[ROWS], colgrid[ROWS];
+    int hidx[ROWS], cidx[ROWS];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < ROWS; ++h) {
         const int lz = lr + 4 * h, z = T.z0 + lz;
         hidx[h] = (lz + 1) * EFM_HX + lx + EFM_HX_OFF;
         cidx[h] = lz * EFM_STX + lx;
@@ -372,10 +383,10 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         const int y = j;
         const bool plane_in = j >= EFM_HS && j < ny - EFM_HS;
         const bool rec_plane = (recbits >> (j - T.ys)) & 1ull;
-        float pp[2][9];
+        float pp[ROWS][9];
         if (PASS != EFM_REV) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
+            for (int h = 0; h < ROWS; ++h)
                 if (plane_in && colin[h]) load_psi<3>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
         }
         const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
@@ -385,7 +396,7 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
             // box interior -> stencil update, never-updated cells -> 0
             const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < ROWS; ++h) {
                 if (!colgrid[h]) continue;
                 const int z = T.z0 + lr + 4 * h;
                 const int hi = hidx[h], ci = cidx[h];
@@ -429,7 +440,7 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         } else if (mine) {
             const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < ROWS; ++h) {
                 const int z = T.z0 + lr + 4 * h;
                 const bool guard = plane_in && colin[h];
                 const bool rec = rec_plane && colgrid[h] && efm_rec_bit(I, x, y, z);
@@ -541,7 +552,7 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         ok = __syncthreads_and(mine) != 0;
         if (!ok) break;
         if (j - 1 + EFM_SR <= last) {
-            if (threadIdx.x == 0) issue_plane<NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
+            if (threadIdx.x == 0) issue_plane<ROWS, NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
             issued_hi = j - 1 + EFM_SR;
         }
     }
@@ -561,24 +572,37 @@ __global__ void efm_model_reciprocals(const float *__restrict__ mu, const float 
 cudaError_t efm_image_init_attributes();
 
 // ---------------------------------------------------------------------------- launchers
-static const size_t kSmemStress = (size_t)EFM_SR * (4 * EFM_HALO_BYTES + 7 * EFM_CENTER_BYTES);
-static const size_t kSmemVelocity = (size_t)EFM_SR * (6 * EFM_HALO_BYTES + 4 * EFM_CENTER_BYTES);
+template <int ROWS>
+constexpr int kSmemStress = efm_stream_smem(ROWS, 4, 7);
+template <int ROWS>
+constexpr int kSmemVelocity = efm_stream_smem(ROWS, 6, 4);
 
-extern "C" cudaError_t efm_launch_stream(int pass, int kind, const EfmInst *insts, int ninst,
-                                         int tiles, int it, cudaStream_t s) {
+template <int ROWS>
+static void launch_rows(int pass, int kind, const EfmInst *insts, int ninst, int tiles, int it,
+                        cudaStream_t s) {
     if (kind == 0) {
         switch (pass) {
-            case EFM_FWD: efm_stress_stream<EFM_FWD><<<tiles, EFM_STHREADS, kSmemStress, s>>>(insts, ninst, it); break;
-            case EFM_ADJ: efm_stress_stream<EFM_ADJ><<<tiles, EFM_STHREADS, kSmemStress, s>>>(insts, ninst, it); break;
-            default: efm_stress_stream<EFM_REV><<<tiles, EFM_STHREADS, kSmemStress, s>>>(insts, ninst, it); break;
+            case EFM_FWD: efm_stress_stream<EFM_FWD, ROWS><<<tiles, EFM_STHREADS, kSmemStress<ROWS>, s>>>(insts, ninst, it); break;
+            case EFM_ADJ: efm_stress_stream<EFM_ADJ, ROWS><<<tiles, EFM_STHREADS, kSmemStress<ROWS>, s>>>(insts, ninst, it); break;
+            default: efm_stress_stream<EFM_REV, ROWS><<<tiles, EFM_STHREADS, kSmemStress<ROWS>, s>>>(insts, ninst, it); break;
         }
     } else {
         switch (pass) {
-            case EFM_FWD: efm_velocity_stream<EFM_FWD><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
-            case EFM_ADJ: efm_velocity_stream<EFM_ADJ><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
-            default: efm_velocity_stream<EFM_REV><<<tiles, EFM_STHREADS, kSmemVelocity, s>>>(insts, ninst, it); break;
+            case EFM_FWD: efm_velocity_stream<EFM_FWD, ROWS><<<tiles, EFM_STHREADS, kSmemVelocity<ROWS>, s>>>(insts, ninst, it); break;
+            case EFM_ADJ: efm_velocity_stream<EFM_ADJ, ROWS><<<tiles, EFM_STHREADS, kSmemVelocity<ROWS>, s>>>(insts, ninst, it); break;
+            default: efm_velocity_stream<EFM_REV, ROWS><<<tiles, EFM_STHREADS, kSmemVelocity<ROWS>, s>>>(insts, ninst, it); break;
         }
     }
+}
+
+// kind 0 = stress, 1 = velocity; rows = cells per thread (1 or 2), matching the tile layout
+// and tensor-map boxes the table was built with.
+extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, const EfmInst *insts,
+                                         int ninst, int tiles, int it, cudaStream_t s) {
+    if (rows == 1)
+        launch_rows<1>(pass, kind, insts, ninst, tiles, it, s);
+    else
+        launch_rows<2>(pass, kind, insts, ninst, tiles, it, s);
     return cudaGetLastError();
 }
 
@@ -590,14 +614,22 @@ extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho,
     return cudaGetLastError();
 }
 
+template <int ROWS>
+static cudaError_t set_rows_attributes() {
+    cudaError_t e;
+    const int ss = kSmemStress<ROWS>, sv = kSmemVelocity<ROWS>;
+    const auto A = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_FWD, ROWS>, A, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_ADJ, ROWS>, A, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_REV, ROWS>, A, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD, ROWS>, A, sv))) return e;
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ, ROWS>, A, sv))) return e;
+    return cudaFuncSetAttribute(efm_velocity_stream<EFM_REV, ROWS>, A, sv);
+}
+
 extern "C" cudaError_t efm_stream_init_attributes() {
     cudaError_t e;
-    const int ss = (int)kSmemStress, sv = (int)kSmemVelocity;
-    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss))) return e;
-    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss))) return e;
-    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_REV>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss))) return e;
-    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
-    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
-    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_REV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+    if ((e = set_rows_attributes<1>())) return e;
+    if ((e = set_rows_attributes<2>())) return e;
     return efm_image_init_attributes();
 }

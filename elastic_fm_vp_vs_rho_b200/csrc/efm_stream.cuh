@@ -1,15 +1,27 @@
 // Geometry of the plane-streaming kernels (efm_stream.cu).
+//
+// A block owns a 64-wide (x) column of 4 * ROWS z-rows and marches along y; each of its 256
+// threads computes ROWS cells per plane (rows r, r + 4, ...).  ROWS = 2 (64 x 8 tiles, two
+// blocks per SM) and ROWS = 1 (64 x 4 tiles, three blocks per SM) are built.
 #pragma once
 
 #define EFM_STX 64          // tile width along x (cells) = threads per z-row
-#define EFM_STZ 8           // tile rows along z; each thread computes rows r and r + 4
+#define EFM_STZ 8           // tile rows along z of the two-row variant
 #define EFM_STHREADS 256
 #define EFM_SR 4            // ring depth: planes j-1, j, j+1 resident, j+2 in flight
 #define EFM_HX 72           // halo box width: x0-4 .. x0+67 (TMA x start stays 16-byte aligned)
 #define EFM_HX_OFF 4
-#define EFM_HZ 10           // halo box rows: z0-1 .. z0+8
-#define EFM_HALO_TX (EFM_HX * EFM_HZ * 4)        // bytes one halo tile transfers (2880)
-#define EFM_HALO_BYTES 2944                      // ... padded to a 128-byte multiple
-#define EFM_CENTER_TX (EFM_STX * EFM_STZ * 4)    // bytes one cell tile transfers (2048)
-#define EFM_CENTER_BYTES EFM_CENTER_TX
+#define EFM_REC_TZ 4        // z granularity of the per-tile receiver map
 #define EFM_MAX_YCHUNK 64   // planes per block (bit mask of receiver planes is 64 bits)
+
+// Box and shared-memory sizes of the variant computing `rows` cells per thread.
+__host__ __device__ constexpr int efm_st_tz(int rows) { return 4 * rows; }
+__host__ __device__ constexpr int efm_st_hz(int rows) { return 4 * rows + 2; }  // z0-1 .. z0+tz
+__host__ __device__ constexpr int efm_halo_tx(int rows) { return EFM_HX * efm_st_hz(rows) * 4; }
+__host__ __device__ constexpr int efm_halo_bytes(int rows) {
+    return (efm_halo_tx(rows) + 127) / 128 * 128;
+}
+__host__ __device__ constexpr int efm_center_bytes(int rows) { return EFM_STX * efm_st_tz(rows) * 4; }
+__host__ __device__ constexpr int efm_stream_smem(int rows, int nh, int nc) {
+    return EFM_SR * (nh * efm_halo_bytes(rows) + nc * efm_center_bytes(rows));
+}

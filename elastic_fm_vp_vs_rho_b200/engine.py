@@ -61,6 +61,7 @@ class ShotBatch:
         check(self._L.efm_create(ctypes.byref(self._ctx)))
         self.infos: list[InstanceInfo] = []
         self._keep: list[dict] = []
+        self.specs: list[dict] = []  # host-side arguments of add(), for probes / re-creation
 
     # ------------------------------------------------------------------ lifecycle
     def close(self):
@@ -78,6 +79,7 @@ class ShotBatch:
         check(self._L.efm_clear(self._ctx))
         self.infos.clear()
         self._keep.clear()
+        self.specs.clear()
 
     def __len__(self):
         return len(self.infos)
@@ -122,6 +124,8 @@ class ShotBatch:
         info = InstanceInfo(nx, ny, nz, lenpml, float(dx), float(dt), nt, len(src), len(rec))
         self.infos.append(info)
         self._keep.append(dict(lam=lam, mu=mu, rho=rho, wav=wav))
+        self.specs.append(dict(nx=nx, ny=ny, nz=nz, lenpml=lenpml, dx=float(dx), dt=float(dt),
+                               nt=nt, cpml=cp, src=src, mt=mt, rec=rec))
         for i, inf in enumerate(self.infos):
             inf.gather_off = int(self._L.efm_gather_offset(self._ctx, i))
         return iid.value
@@ -132,7 +136,8 @@ class ShotBatch:
         self._keep[i].update(lam=lam, mu=mu, rho=rho)
 
     def set_option(self, option, value):
-        """efm_set_option: _lib.EFM_OPT_STREAM_KERNELS (1/0) or _lib.EFM_OPT_YCHUNK (planes)."""
+        """efm_set_option: _lib.EFM_OPT_STREAM_KERNELS (1/0), _lib.EFM_OPT_YCHUNK (planes),
+        _lib.EFM_OPT_CHECKPOINT_EVERY (steps) or _lib.EFM_OPT_TILE_ROWS (0/1/2)."""
         check(self._L.efm_set_option(self._ctx, int(option), int(value)))
 
     def status(self, stream=None):

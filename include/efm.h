@@ -189,6 +189,9 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 /* Steps between full-state checkpoints of EFM_SAVE_CHECKPOINTS (default 50); memory per
  * instance ~ (nt/K) checkpoints + (K+1) stored steps of the 9 fields. */
 #define EFM_OPT_CHECKPOINT_EVERY 3
+/* Cells per thread of the plane-streaming stress/velocity kernels: 2 (64 x 8 tiles, two
+ * blocks per SM) or 1 (64 x 4 tiles, three blocks per SM); 0 (default) = 2. */
+#define EFM_OPT_TILE_ROWS 4
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*

@@ -291,11 +291,12 @@ def test_receivers_on_never_updated_cells(golden_c1scale, cuda):
     assert rel_err(m[0, 0].cpu().numpy(), gm) < TOL_MT
 
 
-@pytest.mark.parametrize("ychunk", [0, 5, 64])
-def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychunk):
+@pytest.mark.parametrize("ychunk,rows", [(0, 2), (5, 2), (64, 2), (0, 1), (7, 1)])
+def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychunk, rows):
     """TMA plane-streaming kernels = one-thread-per-cell kernels (same arithmetic up to the
     hardware reciprocal in the harmonic means), for the forward, the adjoint, the reverse
-    rebuild and the MT gradient; several chunk lengths."""
+    rebuild and the MT gradient; several chunk lengths and both tile heights (64 x 8 tiles
+    with two cells per thread, 64 x 4 with one)."""
     from elastic_fm_vp_vs_rho_b200 import _lib
     d = golden_c1scale
     out = []
@@ -303,6 +304,7 @@ def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychu
         b = _batch(d, d["lam0"], d["mu0"], d["rho0"], d["mt_obs"])
         b.set_option(_lib.EFM_OPT_STREAM_KERNELS, stream)
         b.set_option(_lib.EFM_OPT_YCHUNK, ychunk)
+        b.set_option(_lib.EFM_OPT_TILE_ROWS, rows)
         mod = b.forward(save_borders=True)
         res, _ = b.residual_misfit(mod, cuda.as_tensor(d["obs0"].reshape(-1)).cuda())
         g, m = b.gradient(res, model=True, mt=True)

@@ -59,6 +59,12 @@ class InstanceDesc(ctypes.Structure):
     ]
 
 
+class ConvDesc(ctypes.Structure):
+    """Mirror of efm_conv_desc."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("cin", ctypes.c_int), ("cout", ctypes.c_int)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _L = ctypes.c_int64
@@ -91,6 +97,14 @@ SIGNATURES = {
     "efm_lbfgs_direction": (_I, [_P, _P, _P, _P, _P, _I, _L, _I, _P]),
     "efm_smooth_mask": (_I, [_P, _P, _I, _I, _I, _F, _I, _I, _P]),
     "efm_chain_rule": (_I, [_P, _P, _P, _P, _P, _P, _L, _P]),
+    "efm_conv3d_supported": (_I, [_I, _I]),
+    "efm_conv3d_prep_weights": (_I, [_I, _I, _P, _P, _P, _P]),
+    "efm_conv3d_forward": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _I, _P, _P, _P]),
+    "efm_conv3d_backward_data": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _P, _P]),
+    "efm_conv3d_wgrad_workspace": (ctypes.c_size_t, [ctypes.POINTER(ConvDesc)]),
+    "efm_conv3d_backward_weights": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _P, _P,
+                                         ctypes.c_size_t, _P]),
+    "efm_conv3d_status": (_I, [_P]),
 }
 
 _lock = threading.Lock()

@@ -1,0 +1,666 @@
+// 3x3x3 convolutions of the learned preconditioner as BF16 implicit GEMMs on tcgen05.
+//
+// No counterpart in the reference (it preconditions with a Gaussian filter and L-BFGS);
+// these kernels carry the small 3-D convolutional network that maps gradient volumes to a
+// preconditioned model update.  Volumes are channels-last BF16, element (y, z, x, c) at
+// ((y * nz + z) * nx + x) * C + c, i.e. the modelling grid's (ny, nz, nx) with the channel
+// innermost; padding is "same" (zeros outside the grid), stride 1.  Weights are
+// [27][cout][cin] with tap t = 9 kd + 3 kh + kw reading input (y + kd - 1, z + kh - 1,
+// x + kw - 1).
+//
+// forward / data gradient  (efm_conv_fwd_kernel)
+//   GEMM: M = 128 voxels along x, N = cout, K = 27 cin.  All 27 weight taps stay resident
+//   in shared memory (loaded by TMA once per block).  The block walks its tiles; for each
+//   tile the nine (kd, kh) input rows arrive by TMA as K-major slabs of 136 rows (x0-4 ..
+//   x0+131) x 8 channels, and the three kw taps read the same slab at start addresses 3, 4,
+//   5 rows in.  Warp 0 issues TMA, warp 1 issues tcgen05.mma into a double-buffered TMEM
+//   accumulator, warps 2-5 drain TMEM (tcgen05.ld) and apply bias + ReLU (forward) or the
+//   ReLU mask of the layer below (data gradient) while the next tile accumulates.
+//   The data gradient is the forward kernel with cin/cout swapped and the taps mirrored
+//   (weights prepared by efm_conv_prep_kernel).
+//
+// weight gradient  (efm_conv_wgrad_kernel)
+//   GEMM: M = (kd, kh, ci) rows -- 128 / cin (kd, kh) pairs of cin channels per tile --,
+//   N = cout, K = voxels.  Both operands are MN-major slabs read straight from the
+//   channels-last volumes (8 channels x 64 or 72 voxels per TMA box); the three kw taps
+//   again come from start-address shifts of one 72-row input slab, accumulated in three
+//   TMEM column ranges.  Blocks split K; partial sums go to a workspace and a second kernel
+//   reduces them in a fixed order (deterministic).
+//
+// Every mbarrier wait is bounded; a block that gives up sets the error word, waits (bounded)
+// for its own TMA loads and MMAs in flight, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+
+#include "efm.h"
+#include "efm_tma.cuh"
+#include "efm_umma.cuh"
+
+int efm_internal_fail(int code, const char *msg);
+
+namespace {
+
+constexpr int CV_MT = 128;                 // voxels per forward tile (GEMM M)
+constexpr int CV_AROWS = 136;              // forward input slab rows: x0-4 .. x0+131
+constexpr int CV_ASLAB = CV_AROWS * 16;    // bytes of one 8-channel slab
+constexpr int CV_STAGES = 4;
+constexpr int CV_THREADS = 192;            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int CV_MIN_SMEM = 116 * 1024;    // one block per SM: TMEM allocation never waits
+constexpr int WG_K = 64;                   // voxels per weight-gradient K chunk
+constexpr int WG_AROWS = 72;               // x0-4 .. x0+67
+constexpr int WG_ASLAB = WG_AROWS * 16;    // 1152
+constexpr int WG_BSLAB = WG_K * 16;        // 1024
+
+__device__ unsigned int g_conv_err;
+
+struct Sync {
+    uint64_t full[CV_STAGES], empty[CV_STAGES];
+    uint64_t wbar, tfull[2], tempty[2], drain;
+    uint32_t tmem;
+    int abort;
+};
+
+// Bounded wait that also gives up as soon as another role of the block has given up.
+__device__ __forceinline__ bool cv_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    for (uint32_t i = 0; i < EFM_WAIT_LIMIT; ++i) {
+        if (efm_mbar_try_wait(bar, parity)) return true;
+        if ((i & 255u) == 255u && *abort) return false;
+    }
+    *abort = 1;
+    atomicOr(&g_conv_err, EFM_ERR_FLAG_TIMEOUT);
+    return false;
+}
+
+__device__ __forceinline__ void cv_drain_wait(uint64_t *bar, uint32_t parity) {
+    for (uint32_t i = 0; i < EFM_WAIT_LIMIT; ++i)
+        if (efm_mbar_try_wait(bar, parity)) return;
+    atomicOr(&g_conv_err, EFM_ERR_FLAG_TIMEOUT);
+}
+
+// Block set-up common to both kernels: barriers, TMEM allocation (warp 1).
+__device__ __forceinline__ void cv_setup(Sync &S, int epi_count, uint32_t ncols) {
+    const int warp = threadIdx.x / 32;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < CV_STAGES; ++s) {
+            efm_mbar_init(&S.full[s], 1);
+            efm_mbar_init(&S.empty[s], 1);
+        }
+        efm_mbar_init(&S.wbar, 1);
+        for (int b = 0; b < 2; ++b) {
+            efm_mbar_init(&S.tfull[b], 1);
+            efm_mbar_init(&S.tempty[b], epi_count);
+        }
+        efm_mbar_init(&S.drain, 1);
+        S.abort = 0;
+        efm_fence_barrier_init();
+    }
+    if (warp == 1) efm_tmem_alloc(&S.tmem, ncols);
+    efm_tc_fence_before();
+    __syncthreads();
+    efm_tc_fence_after();
+}
+
+// All roles done: the MMA thread waits for its last MMAs, then warp 1 frees TMEM.
+__device__ __forceinline__ void cv_teardown(Sync &S, uint32_t ncols, bool mma_issued) {
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (warp == 1 && lane == 0 && mma_issued) {
+        efm_mma_commit(&S.drain);
+        cv_drain_wait(&S.drain, 0);
+    }
+    efm_tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        efm_tc_fence_after();
+        efm_tmem_free(S.tmem, ncols);
+    }
+}
+
+__device__ __forceinline__ void store_bf16x8(__nv_bfloat16 *dst, const float *v) {
+    uint4 u;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    *reinterpret_cast<uint4 *>(dst) = u;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ forward / data gradient
+// MODE 0: y = act(conv(x) + bias) (bf16 and/or fp32 out); MODE 1: y = conv(x) * [mask > 0].
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(CV_THREADS, 1)
+efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_w,
+                    int nx, int ny, int nz, const float *__restrict__ bias, int relu,
+                    const __nv_bfloat16 *__restrict__ mask, __nv_bfloat16 *__restrict__ y_bf16,
+                    float *__restrict__ y_f32) {
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 64 && CIN <= 64, "channels");
+    constexpr int NG = CIN / 8;                       // 8-channel groups (K core matrices)
+    constexpr int WBYTES = 27 * CIN * COUT * 2;
+    constexpr int ASTAGE = NG * CV_ASLAB;
+    constexpr uint32_t IDESC = efm_idesc_bf16(CV_MT, COUT, false, false);
+    constexpr uint32_t NCOLS = COUT * 2 <= 32 ? 32 : COUT * 2;  // double-buffered accumulator
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ Sync S;
+    unsigned char *wsm = smem;
+    unsigned char *asm_ = smem + WBYTES;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int xt = (nx + CV_MT - 1) / CV_MT;
+    const int ntiles = xt * nz * ny;
+    cv_setup(S, 128, NCOLS);
+    volatile int *abort = &S.abort;
+    bool mma_issued = false;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer
+        efm_prefetch_tmap(&tm_x);
+        efm_prefetch_tmap(&tm_w);
+        efm_mbar_expect_tx(&S.wbar, WBYTES);
+        for (int g = 0; g < NG; ++g)
+            efm_tma_load_3d(wsm + g * 27 * COUT * 16, &tm_w, &S.wbar, 8 * g, 0, 0);
+        int st = 0;
+        uint32_t ph = 0;
+        uint32_t issued_parity[CV_STAGES];
+        bool issued[CV_STAGES] = {};
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int x0 = (tile % xt) * CV_MT, z = (tile / xt) % nz, y = tile / (xt * nz);
+            for (int kk = 0; kk < 9; ++kk) {
+                if (!cv_wait(&S.empty[st], ph ^ 1u, abort)) { ok = false; break; }
+                efm_mbar_expect_tx(&S.full[st], ASTAGE);
+                unsigned char *dst = asm_ + st * ASTAGE;
+                for (int g = 0; g < NG; ++g)
+                    efm_tma_load_4d(dst + g * CV_ASLAB, &tm_x, &S.full[st], 8 * g, x0 - 4,
+                                    z + kk % 3 - 1, y + kk / 3 - 1);
+                issued[st] = true;
+                issued_parity[st] = ph;
+                if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
+            }
+        }
+        if (!ok) {  // no load may still target this block's shared memory
+            for (int s = 0; s < CV_STAGES; ++s)
+                if (issued[s]) cv_drain_wait(&S.full[s], issued_parity[s]);
+        }
+        cv_drain_wait(&S.wbar, 0);
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        bool ok = cv_wait(&S.wbar, 0, abort);
+        const uint32_t wbase = efm_smem_addr(wsm), abase = efm_smem_addr(asm_);
+        int st = 0, acc = 0;
+        uint32_t ph = 0, aph = 0;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            if (!cv_wait(&S.tempty[acc], aph ^ 1u, abort)) { ok = false; break; }
+            efm_tc_fence_after();
+            const uint32_t d = S.tmem + acc * COUT;
+            for (int kk = 0; kk < 9 && ok; ++kk) {
+                if (!cv_wait(&S.full[st], ph, abort)) { ok = false; break; }
+                efm_tc_fence_after();
+                const uint32_t a0 = abase + st * ASTAGE;
+#pragma unroll
+                for (int kw = 0; kw < 3; ++kw) {
+                    const int t = kk * 3 + kw;
+#pragma unroll
+                    for (int j = 0; j < CIN / 16; ++j) {
+                        const uint64_t a = efm_sdesc(a0 + 2 * j * CV_ASLAB + (kw + 3) * 16, CV_ASLAB, 128);
+                        const uint64_t b = efm_sdesc(wbase + (2 * j * 27 + t) * COUT * 16, 27 * COUT * 16, 128);
+                        efm_mma_bf16(d, a, b, IDESC, (kk | kw | j) != 0);
+                    }
+                }
+                mma_issued = true;
+                efm_mma_commit(&S.empty[st]);  // frees the slab once these MMAs have read it
+                if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
+            }
+            if (!ok) break;
+            efm_mma_commit(&S.tfull[acc]);
+            if (++acc == 2) { acc = 0; aph ^= 1u; }
+        }
+    } else if (warp >= 2) {
+        // ---------------- epilogue: TMEM -> registers -> global
+        const int q = warp % 4;           // TMEM lane quadrant this warp may read
+        const int row = q * 32 + lane;    // voxel of the tile
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            if (!cv_wait(&S.tfull[acc], aph, abort)) break;
+            efm_tc_fence_after();
+            float v[COUT];
+#pragma unroll
+            for (int c = 0; c < COUT; c += 16)
+                efm_tmem_ld16(S.tmem + ((uint32_t)(q * 32) << 16) + acc * COUT + c, v + c);
+            efm_tc_fence_before();
+            efm_mbar_arrive(&S.tempty[acc]);
+            if (++acc == 2) { acc = 0; aph ^= 1u; }
+            const int x0 = (tile % xt) * CV_MT, z = (tile / xt) % nz, y = tile / (xt * nz);
+            const int x = x0 + row;
+            if (x >= nx) continue;
+            const int64_t vox = ((int64_t)y * nz + z) * nx + x;
+            if (MODE == 0) {
+#pragma unroll
+                for (int c = 0; c < COUT; ++c) {
+                    float r = v[c] + (bias ? bias[c] : 0.f);
+                    v[c] = (relu && r < 0.f) ? 0.f : r;
+                }
+                if (y_f32) {
+                    float4 *o = reinterpret_cast<float4 *>(y_f32 + vox * COUT);
+#pragma unroll
+                    for (int c = 0; c < COUT; c += 4) o[c / 4] = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                }
+            } else if (mask != nullptr) {
+                const uint4 *m = reinterpret_cast<const uint4 *>(mask + vox * COUT);
+#pragma unroll
+                for (int c = 0; c < COUT; c += 8) {
+                    const uint4 u = m[c / 8];
+                    const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&u);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        if (!(__bfloat162float(h[i]) > 0.f)) v[c + i] = 0.f;
+                }
+            }
+            if (y_bf16) {
+#pragma unroll
+                for (int c = 0; c < COUT; c += 8) store_bf16x8(y_bf16 + vox * COUT + c, v + c);
+            }
+        }
+    }
+    __syncwarp();
+    cv_teardown(S, NCOLS, mma_issued);
+}
+
+// ------------------------------------------------------------------------ weight gradient
+// partial[split][q][kw][128][COUT]: rows (local pair, ci) of M tile q.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CV_THREADS, 1)
+efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_dy,
+                      int nx, int ny, int nz, float *__restrict__ partial) {
+    constexpr int NPAIR = 128 / CIN;               // (kd, kh) pairs per M tile
+    constexpr int NGI = CIN / 8, NGO = COUT / 8;
+    constexpr int ASTAGE = NPAIR * NGI * WG_ASLAB;  // 16 slabs
+    constexpr int BSTAGE = NGO * WG_BSLAB;
+    constexpr int STAGE = ASTAGE + BSTAGE;
+    constexpr uint32_t IDESC = efm_idesc_bf16(128, COUT, true, true);
+    constexpr uint32_t NCOLS = 3 * COUT <= 32 ? 32 : 3 * COUT <= 64 ? 64 : 3 * COUT <= 128 ? 128 : 256;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ Sync S;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int q = blockIdx.y, split = blockIdx.x, nsplit = gridDim.x;
+    const int xc = (nx + WG_K - 1) / WG_K;
+    const int64_t units = (int64_t)xc * nz * ny;
+    const int64_t u0 = units * split / nsplit, u1 = units * (split + 1) / nsplit;
+    cv_setup(S, 128, NCOLS);
+    volatile int *abort = &S.abort;
+    bool mma_issued = false;
+
+    if (warp == 0 && lane == 0) {
+        efm_prefetch_tmap(&tm_x);
+        efm_prefetch_tmap(&tm_dy);
+        int st = 0;
+        uint32_t ph = 0;
+        uint32_t issued_parity[CV_STAGES];
+        bool issued[CV_STAGES] = {};
+        bool ok = true;
+        for (int64_t u = u0; u < u1; ++u) {
+            const int x0 = (int)(u % xc) * WG_K, z = (int)((u / xc) % nz), y = (int)(u / ((int64_t)xc * nz));
+            if (!cv_wait(&S.empty[st], ph ^ 1u, abort)) { ok = false; break; }
+            efm_mbar_expect_tx(&S.full[st], STAGE);
+            unsigned char *dst = smem + st * STAGE;
+            for (int lp = 0; lp < NPAIR; ++lp) {
+                const int pi = q * NPAIR + lp;  // (kd, kh) = (pi / 3, pi % 3); pi > 8: zero rows
+                const int zz = pi < 9 ? z + pi % 3 - 1 : -64;
+                const int yy = pi < 9 ? y + pi / 3 - 1 : -64;
+                for (int g = 0; g < NGI; ++g)
+                    efm_tma_load_4d(dst + (lp * NGI + g) * WG_ASLAB, &tm_x, &S.full[st], 8 * g,
+                                    x0 - 4, zz, yy);
+            }
+            for (int g = 0; g < NGO; ++g)
+                efm_tma_load_4d(dst + ASTAGE + g * WG_BSLAB, &tm_dy, &S.full[st], 8 * g, x0, z, y);
+            issued[st] = true;
+            issued_parity[st] = ph;
+            if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
+        }
+        if (!ok)
+            for (int s = 0; s < CV_STAGES; ++s)
+                if (issued[s]) cv_drain_wait(&S.full[s], issued_parity[s]);
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t base = efm_smem_addr(smem);
+        int st = 0;
+        uint32_t ph = 0;
+        bool ok = true;
+        for (int64_t u = u0; u < u1; ++u) {
+            if (!cv_wait(&S.full[st], ph, abort)) { ok = false; break; }
+            efm_tc_fence_after();
+            const uint32_t a0 = base + st * STAGE, b0 = a0 + ASTAGE;
+#pragma unroll
+            for (int kw = 0; kw < 3; ++kw) {
+#pragma unroll
+                for (int j = 0; j < WG_K / 16; ++j) {
+                    const uint64_t a = efm_sdesc(a0 + 256 * j + (kw + 3) * 16, 128, WG_ASLAB);
+                    const uint64_t b = efm_sdesc(b0 + 256 * j, 128, WG_BSLAB);
+                    efm_mma_bf16(S.tmem + kw * COUT, a, b, IDESC, (u != u0 || j != 0) ? 1u : 0u);
+                }
+            }
+            mma_issued = true;
+            efm_mma_commit(&S.empty[st]);
+            if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
+        }
+        if (ok && mma_issued) efm_mma_commit(&S.tfull[0]);
+    } else if (warp >= 2) {
+        const int qd = warp % 4, row = qd * 32 + lane;
+        bool have = u1 > u0;
+        if (have && !cv_wait(&S.tfull[0], 0, abort)) have = false;
+        if (u1 > u0 && !have) {
+            // gave up: leave the partial untouched (the error word reports it)
+        } else {
+            efm_tc_fence_after();
+            float *out = partial + ((((int64_t)split * gridDim.y + q) * 3) * 128 + row) * COUT;
+#pragma unroll
+            for (int kw = 0; kw < 3; ++kw) {
+                float v[COUT];
+                if (have) {
+#pragma unroll
+                    for (int c = 0; c < COUT; c += 16)
+                        efm_tmem_ld16(S.tmem + ((uint32_t)(qd * 32) << 16) + kw * COUT + c, v + c);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < COUT; ++c) v[c] = 0.f;
+                }
+                float4 *o = reinterpret_cast<float4 *>(out + (int64_t)kw * 128 * COUT);
+#pragma unroll
+                for (int c = 0; c < COUT; c += 4) o[c / 4] = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+            }
+        }
+    }
+    __syncwarp();
+    cv_teardown(S, NCOLS, mma_issued);
+}
+
+// dw[t][co][ci] = sum over splits (fixed order) of the partial rows; t = 3 pi + kw.
+__global__ void efm_conv_wgrad_reduce(const float *__restrict__ partial, int nsplit, int nq,
+                                      int cin, int cout, float *__restrict__ dw) {
+    const int n = 27 * cout * cin;
+    const int npair = 128 / cin;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int ci = i % cin, co = (i / cin) % cout, t = i / (cin * cout);
+        const int pi = t / 3, kw = t % 3, qq = pi / npair, lp = pi % npair;
+        const int row = lp * cin + ci;
+        double s = 0.0;
+        for (int sp = 0; sp < nsplit; ++sp)
+            s += partial[((((int64_t)sp * nq + qq) * 3 + kw) * 128 + row) * cout + co];
+        dw[i] = (float)s;
+    }
+}
+
+// db[co] = sum over voxels of dy[., co]: per-block partial sums, then a fixed-order total.
+__global__ void efm_conv_bias_partial(const __nv_bfloat16 *__restrict__ dy, int64_t nvox, int cout,
+                                      float *__restrict__ part) {
+    // block b, thread (c, r): channel c = threadIdx.x % cout, voxel lane r = threadIdx.x / cout
+    const int c = threadIdx.x % cout, r = threadIdx.x / cout, nr = blockDim.x / cout;
+    float s = 0.f;
+    for (int64_t v = (int64_t)blockIdx.x * nr + r; v < nvox; v += (int64_t)gridDim.x * nr)
+        s += __bfloat162float(dy[v * cout + c]);
+    extern __shared__ float red[];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    if (r == 0) {
+        float t = 0.f;
+        for (int k = 0; k < nr; ++k) t += red[k * cout + c];
+        part[(int64_t)blockIdx.x * cout + c] = t;
+    }
+}
+
+__global__ void efm_conv_bias_final(const float *__restrict__ part, int nblocks, int cout,
+                                    float *__restrict__ db) {
+    const int c = threadIdx.x;
+    if (c >= cout) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += part[(int64_t)b * cout + c];
+    db[c] = (float)s;
+}
+
+// fp32 [27][cout][cin] -> bf16 forward weights and bf16 mirrored transpose [27][cin][cout]
+// (w_t[26 - t][ci][co] = w[t][co][ci]) for the data gradient.
+__global__ void efm_conv_prep_kernel(const float *__restrict__ w, int cin, int cout,
+                                     __nv_bfloat16 *__restrict__ wb, __nv_bfloat16 *__restrict__ wt) {
+    const int n = 27 * cin * cout;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int ci = i % cin, co = (i / cin) % cout, t = i / (cin * cout);
+        const __nv_bfloat16 b = __float2bfloat16_rn(w[i]);
+        if (wb) wb[i] = b;
+        if (wt) wt[((int64_t)(26 - t) * cin + ci) * cout + co] = b;
+    }
+}
+
+// ============================================================================ host side
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 conv_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// channels-last BF16 volume (ny, nz, nx, c); box (8 channels, rows along x, 1, 1)
+int map_volume(CUtensorMap *m, const void *base, const efm_conv_desc *d, int c, int rows) {
+    auto enc = conv_encoder();
+    if (!enc) return efm_internal_fail(EFM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)d->nx, (cuuint64_t)d->nz, (cuuint64_t)d->ny};
+    cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * d->nx,
+                             (cuuint64_t)c * 2 * d->nx * d->nz};
+    cuuint32_t box[4] = {8, (cuuint32_t)rows, 1, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides,
+                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return efm_internal_fail(EFM_ERR_CUDA, ("tensor map (volume) failed: " + std::to_string((int)r)).c_str());
+    return EFM_OK;
+}
+
+// weights [27][cout][cin] BF16; box (8, cout, 27)
+int map_weights(CUtensorMap *m, const void *base, int cin, int cout) {
+    auto enc = conv_encoder();
+    if (!enc) return efm_internal_fail(EFM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[3] = {(cuuint64_t)cin, (cuuint64_t)cout, 27};
+    cuuint64_t strides[2] = {(cuuint64_t)cin * 2, (cuuint64_t)cin * cout * 2};
+    cuuint32_t box[3] = {8, (cuuint32_t)cout, 27};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides,
+                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return efm_internal_fail(EFM_ERR_CUDA, ("tensor map (weights) failed: " + std::to_string((int)r)).c_str());
+    return EFM_OK;
+}
+
+bool chan_ok(int c) { return c == 16 || c == 32 || c == 64; }
+
+int check_desc(const efm_conv_desc *d) {
+    if (d == nullptr) return efm_internal_fail(EFM_ERR_ARG, "null conv descriptor");
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1) return efm_internal_fail(EFM_ERR_ARG, "empty volume");
+    if (!chan_ok(d->cin) || !chan_ok(d->cout))
+        return efm_internal_fail(EFM_ERR_ARG, "channels must be 16, 32 or 64");
+    if (d->cin == 64 && d->cout == 64)
+        return efm_internal_fail(EFM_ERR_ARG, "64 -> 64 channels: weights exceed shared memory");
+    return EFM_OK;
+}
+
+bool al16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int num_sms() {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
+template <int CIN, int COUT, int MODE>
+int launch_fwd(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tw, const float *bias,
+               int relu, const void *mask, void *yb, float *yf, cudaStream_t s) {
+    const int smem_need = 27 * CIN * COUT * 2 + CV_STAGES * (CIN / 8) * CV_ASLAB;
+    const int smem = smem_need > CV_MIN_SMEM ? smem_need : CV_MIN_SMEM;
+    auto k = efm_conv_fwd_kernel<CIN, COUT, MODE>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+    const int64_t tiles = (int64_t)((d->nx + CV_MT - 1) / CV_MT) * d->nz * d->ny;
+    const int grid = (int)(tiles < num_sms() ? tiles : num_sms());
+    k<<<grid, CV_THREADS, smem, s>>>(tx, tw, d->nx, d->ny, d->nz, bias, relu,
+                                      static_cast<const __nv_bfloat16 *>(mask),
+                                      static_cast<__nv_bfloat16 *>(yb), yf);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+}
+
+template <int MODE>
+int dispatch_fwd(int cin, int cout, const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tw,
+                 const float *bias, int relu, const void *mask, void *yb, float *yf, cudaStream_t s) {
+#define EFM_CONV_CASE(A, B)                                                           \
+    if (cin == A && cout == B)                                                        \
+        return launch_fwd<A, B, MODE>(d, tx, tw, bias, relu, mask, yb, yf, s);
+    EFM_CONV_CASE(16, 16) EFM_CONV_CASE(16, 32) EFM_CONV_CASE(16, 64)
+    EFM_CONV_CASE(32, 16) EFM_CONV_CASE(32, 32) EFM_CONV_CASE(32, 64)
+    EFM_CONV_CASE(64, 16) EFM_CONV_CASE(64, 32)
+#undef EFM_CONV_CASE
+    return efm_internal_fail(EFM_ERR_ARG, "unsupported channel pair");
+}
+
+int wgrad_splits(const efm_conv_desc *d, int nq) {
+    const int64_t units = (int64_t)((d->nx + WG_K - 1) / WG_K) * d->nz * d->ny;
+    int64_t s = (num_sms() + nq - 1) / nq;
+    if (s > units) s = units;
+    return (int)(s < 1 ? 1 : s);
+}
+
+int wgrad_nq(int cin) { return (9 + 128 / cin - 1) / (128 / cin); }
+
+template <int CIN, int COUT>
+int launch_wgrad(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tdy, float *part,
+                 int nsplit, cudaStream_t s) {
+    constexpr int stage = (128 / CIN) * (CIN / 8) * WG_ASLAB + (COUT / 8) * WG_BSLAB;
+    const int smem_need = CV_STAGES * stage;
+    const int smem = smem_need > CV_MIN_SMEM ? smem_need : CV_MIN_SMEM;
+    auto k = efm_conv_wgrad_kernel<CIN, COUT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+    dim3 grid(nsplit, wgrad_nq(CIN));
+    k<<<grid, CV_THREADS, smem, s>>>(tx, tdy, d->nx, d->ny, d->nz, part);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+}
+
+constexpr int BIAS_BLOCKS = 296;
+
+}  // namespace
+
+extern "C" {
+
+int efm_conv3d_supported(int cin, int cout) {
+    return chan_ok(cin) && chan_ok(cout) && !(cin == 64 && cout == 64);
+}
+
+int efm_conv3d_prep_weights(int cin, int cout, const float *w, void *w_bf16, void *wt_bf16, void *stream) {
+    if (!efm_conv3d_supported(cin, cout)) return efm_internal_fail(EFM_ERR_ARG, "unsupported channel pair");
+    if (w == nullptr) return efm_internal_fail(EFM_ERR_ARG, "null weights");
+    efm_conv_prep_kernel<<<64, 256, 0, (cudaStream_t)stream>>>(
+        w, cin, cout, static_cast<__nv_bfloat16 *>(w_bf16), static_cast<__nv_bfloat16 *>(wt_bf16));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int efm_conv3d_forward(const efm_conv_desc *d, const void *x, const void *w_bf16, const float *bias,
+                       int relu, void *y_bf16, float *y_f32, void *stream) {
+    int rc;
+    if ((rc = check_desc(d))) return rc;
+    if (!x || !w_bf16 || (!y_bf16 && !y_f32)) return efm_internal_fail(EFM_ERR_ARG, "null pointer");
+    if (!al16(x) || !al16(w_bf16) || !al16(y_bf16) || !al16(y_f32))
+        return efm_internal_fail(EFM_ERR_ARG, "buffers must be 16-byte aligned");
+    CUtensorMap tx, tw;
+    if ((rc = map_volume(&tx, x, d, d->cin, CV_AROWS))) return rc;
+    if ((rc = map_weights(&tw, w_bf16, d->cin, d->cout))) return rc;
+    return dispatch_fwd<0>(d->cin, d->cout, d, tx, tw, bias, relu, nullptr, y_bf16, y_f32,
+                           (cudaStream_t)stream);
+}
+
+int efm_conv3d_backward_data(const efm_conv_desc *d, const void *dy, const void *wt_bf16,
+                             const void *relu_mask, void *dx, void *stream) {
+    int rc;
+    if ((rc = check_desc(d))) return rc;
+    if (!dy || !wt_bf16 || !dx) return efm_internal_fail(EFM_ERR_ARG, "null pointer");
+    if (!al16(dy) || !al16(wt_bf16) || !al16(dx) || !al16(relu_mask))
+        return efm_internal_fail(EFM_ERR_ARG, "buffers must be 16-byte aligned");
+    efm_conv_desc t = *d;
+    t.cin = d->cout;
+    t.cout = d->cin;
+    CUtensorMap tx, tw;
+    if ((rc = map_volume(&tx, dy, &t, t.cin, CV_AROWS))) return rc;
+    if ((rc = map_weights(&tw, wt_bf16, t.cin, t.cout))) return rc;
+    return dispatch_fwd<1>(t.cin, t.cout, &t, tx, tw, nullptr, 0, relu_mask, dx, nullptr,
+                           (cudaStream_t)stream);
+}
+
+size_t efm_conv3d_wgrad_workspace(const efm_conv_desc *d) {
+    if (check_desc(d)) return 0;
+    const int nq = wgrad_nq(d->cin);
+    const size_t part = (size_t)wgrad_splits(d, nq) * nq * 3 * 128 * d->cout * sizeof(float);
+    return part + (size_t)BIAS_BLOCKS * d->cout * sizeof(float);
+}
+
+int efm_conv3d_backward_weights(const efm_conv_desc *d, const void *x, const void *dy, float *dw,
+                                float *db, void *workspace, size_t ws_bytes, void *stream) {
+    int rc;
+    if ((rc = check_desc(d))) return rc;
+    if (!x || !dy || !dw || !workspace) return efm_internal_fail(EFM_ERR_ARG, "null pointer");
+    if (ws_bytes < efm_conv3d_wgrad_workspace(d)) return efm_internal_fail(EFM_ERR_ARG, "workspace too small");
+    if (!al16(x) || !al16(dy) || !al16(workspace))
+        return efm_internal_fail(EFM_ERR_ARG, "buffers must be 16-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    CUtensorMap tx, tdy;
+    if ((rc = map_volume(&tx, x, d, d->cin, WG_AROWS))) return rc;
+    if ((rc = map_volume(&tdy, dy, d, d->cout, WG_K))) return rc;
+    const int nq = wgrad_nq(d->cin), nsplit = wgrad_splits(d, nq);
+    float *part = static_cast<float *>(workspace);
+    rc = EFM_ERR_ARG;
+#define EFM_WG_CASE(A, B) \
+    if (d->cin == A && d->cout == B) rc = launch_wgrad<A, B>(d, tx, tdy, part, nsplit, s);
+    EFM_WG_CASE(16, 16) EFM_WG_CASE(16, 32) EFM_WG_CASE(16, 64)
+    EFM_WG_CASE(32, 16) EFM_WG_CASE(32, 32) EFM_WG_CASE(32, 64)
+    EFM_WG_CASE(64, 16) EFM_WG_CASE(64, 32)
+#undef EFM_WG_CASE
+    if (rc) return rc;
+    efm_conv_wgrad_reduce<<<64, 256, 0, s>>>(part, nsplit, nq, d->cin, d->cout, dw);
+    if (db) {
+        float *bp = part + (size_t)nsplit * nq * 3 * 128 * d->cout;
+        const int64_t nvox = (int64_t)d->nx * d->ny * d->nz;
+        efm_conv_bias_partial<<<BIAS_BLOCKS, 256, 256 * sizeof(float), s>>>(
+            static_cast<const __nv_bfloat16 *>(dy), nvox, d->cout, bp);
+        efm_conv_bias_final<<<1, 64, 0, s>>>(bp, BIAS_BLOCKS, d->cout, db);
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int efm_conv3d_status(void *stream) {
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+    unsigned int h = 0;
+    if ((e = cudaMemcpyFromSymbol(&h, g_conv_err, sizeof(h))) != cudaSuccess)
+        return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
+    if (h) {
+        const unsigned int z = 0;
+        cudaMemcpyToSymbol(g_conv_err, &z, sizeof(z));
+        return efm_internal_fail(EFM_ERR_TIMEOUT, "a convolution kernel gave up a bounded wait");
+    }
+    return EFM_OK;
+}
+
+}  // extern "C"

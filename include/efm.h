@@ -264,6 +264,49 @@ EFM_API int efm_smooth_mask(float *g_dev, float *tmp_dev, int nx, int ny, int nz
 EFM_API int efm_chain_rule(float *g_lam_dev, float *g_mu_dev, float *g_rho_dev, const float *vp_dev,
                    const float *vs_dev, const float *rho_dev, int64_t n, void *stream);
 
+/* ------------------------------------------------ learned preconditioner: 3x3x3 conv3d
+ *
+ * No counterpart in the reference (which preconditions with gaussian_filter and L-BFGS,
+ * mainPropElastic3D_MT.py:2479-2504, lbfgs.py:27-67): these carry a small 3-D
+ * convolutional network that maps gradient volumes to a model update.  BF16 operands,
+ * FP32 accumulation on the tcgen05 tensor cores (implicit GEMM, TMA-fed).
+ *
+ * Volumes are channels-last BF16 on the device: element (y, z, x, c) of an (ny, nz, nx)
+ * grid at ((y nz + z) nx + x) C + c.  Weights are [27][cout][cin] with tap
+ * t = 9 kd + 3 kh + kw reading (y + kd - 1, z + kh - 1, x + kw - 1); zero padding, stride 1
+ * (torch.nn.functional.conv3d(padding=1) of the (1, C, ny, nz, nx) tensor with weight
+ * w[co][ci][kd][kh][kw]).  Channels: 16, 32 or 64 (not 64 -> 64).  All buffers 16-byte
+ * aligned.  Kernels that give up a bounded wait report it through efm_conv3d_status.
+ */
+typedef struct efm_conv_desc {
+    int nx, ny, nz;  /* grid */
+    int cin, cout;   /* channels of the forward layer */
+} efm_conv_desc;
+
+EFM_API int efm_conv3d_supported(int cin, int cout);
+/* fp32 [27][cout][cin] -> BF16 forward weights (same layout) and BF16 data-gradient weights
+ * [27][cin][cout] with the taps mirrored; either output may be NULL. */
+EFM_API int efm_conv3d_prep_weights(int cin, int cout, const float *w_dev, void *w_bf16_dev,
+                                    void *wt_bf16_dev, void *stream);
+/* y = act(conv(x) + bias); act = ReLU when relu != 0.  Writes y_bf16 [.., cout] and/or
+ * y_f32 [.., cout] (either may be NULL, not both); bias may be NULL. */
+EFM_API int efm_conv3d_forward(const efm_conv_desc *d, const void *x_dev, const void *w_bf16_dev,
+                               const float *bias_dev, int relu, void *y_bf16_dev, float *y_f32_dev,
+                               void *stream);
+/* dx = conv^T(dy) [.., cin], times [relu_mask > 0] when relu_mask ([.., cin], the layer's
+ * input = the output of the ReLU below) is not NULL.  wt: the mirrored weights. */
+EFM_API int efm_conv3d_backward_data(const efm_conv_desc *d, const void *dy_dev,
+                                     const void *wt_bf16_dev, const void *relu_mask_dev,
+                                     void *dx_dev, void *stream);
+/* dw [27][cout][cin] (fp32, overwritten) = sum over voxels of dy x shifted input;
+ * db [cout] (fp32, overwritten, may be NULL) = sum of dy.  Deterministic order. */
+EFM_API size_t efm_conv3d_wgrad_workspace(const efm_conv_desc *d);
+EFM_API int efm_conv3d_backward_weights(const efm_conv_desc *d, const void *x_dev,
+                                        const void *dy_dev, float *dw_dev, float *db_dev,
+                                        void *workspace_dev, size_t workspace_bytes, void *stream);
+/* Synchronizes `stream`; EFM_ERR_TIMEOUT if a convolution kernel gave up a wait (cleared). */
+EFM_API int efm_conv3d_status(void *stream);
+
 #ifdef __cplusplus
 }
 #endif

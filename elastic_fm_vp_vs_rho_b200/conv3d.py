@@ -105,3 +105,52 @@ def backward_weights(x, dy, workspace=None, stream=None, with_bias=True):
 def status(stream=None):
     """Raise EfmError(EFM_ERR_TIMEOUT) if a convolution kernel gave up a wait (synchronizes)."""
     check(_lib.load().efm_conv3d_status(stream_ptr(stream)))
+
+
+def bench(shape=(128, 128, 256), pairs=((16, 32), (32, 64), (64, 32), (32, 16)), reps=5,
+          warmup=2):
+    """Device time and tensor throughput of forward / data-gradient / weight-gradient launches
+    (CUDA events on the launching stream).  FLOPs per launch: 2 x 27 x cin x cout x voxels."""
+    import torch
+    ny, nz, nx = shape
+    nvox = ny * nz * nx
+    out = []
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for cin, cout in pairs:
+        x = torch.randn(shape + (cin,), device="cuda", generator=g).to(torch.bfloat16)
+        dy = torch.randn(shape + (cout,), device="cuda", generator=g).to(torch.bfloat16)
+        w = torch.randn((27, cout, cin), device="cuda", generator=g) * 0.05
+        b = torch.zeros(cout, device="cuda")
+        wb, wt = prep_weights(w)
+        ws = WgradWorkspace()
+        flops = 2.0 * 27 * cin * cout * nvox
+        row = dict(cin=cin, cout=cout, voxels=nvox, gflop=flops / 1e9)
+        cases = {
+            "forward": lambda: forward(x, wb, b, relu=True),
+            "backward_data": lambda: backward_data(dy, wt, cin, relu_mask=x),
+            "backward_weights": lambda: backward_weights(x, dy, ws),
+        }
+        for name, fn in cases.items():
+            for _ in range(warmup):
+                fn()
+            s = torch.cuda.current_stream()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(s)
+            for _ in range(reps):
+                fn()
+            e1.record(s)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            row[name] = dict(ms=ms, tflops=flops / (ms * 1e-3) / 1e12)
+        status()
+        out.append(row)
+    return out
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+    shp = tuple(int(v) for v in sys.argv[1].split(",")) if len(sys.argv) > 1 else (128, 128, 256)
+    for r in bench(shp):
+        print(json.dumps(r))

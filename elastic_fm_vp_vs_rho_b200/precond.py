@@ -1,0 +1,476 @@
+"""Learned preconditioner for the Vp/Vs/rho inversion (no counterpart in the reference).
+
+The reference preconditions its gradients with a Gaussian filter and margin masks
+(mainPropElastic3D_MT.py:2479-2504) and takes L-BFGS steps (lbfgs.py:27-67) after two
+fixed-length steps.  Here a small 3-D convolutional network maps the current gradient and
+model to a model update:
+
+    features (16 channels, channels-last BF16 volume):
+        0-2  gradient of the misfit w.r.t. (Vp, Vs, rho) in normalised units, each scaled
+             by its largest magnitude
+        3-5  the normalised model (value / mean - 1)
+        6    depth z / nz (geometric spreading / illumination falls with depth)
+    network: conv3d 16->32, ReLU, 32->64, ReLU, 64->32, ReLU, 32->16 (3x3x3, zero padding;
+             BF16 tcgen05 kernels of efm_conv.cu with FP32 accumulation)
+    output:  channels 0-2 = the update direction for (Vp, Vs, rho) in normalised units.
+
+Training pairs come from plain L-BFGS runs on seeded random models (the accepted update of
+each iteration, scaled to unit maximum); the loss is the mean squared error over the three
+used channels; Adam on FP32 master weights.
+
+:func:`invert` runs an inversion with either plain L-BFGS or the learned direction; every
+learned direction must pass a descent test (g . d < 0) and an Armijo backtracking line
+search, otherwise that iteration falls back to the plain L-BFGS direction.  Solves are
+counted as in the reference's loop: a gradient costs one forward and one adjoint solve, a
+line-search trial one forward solve.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import conv3d
+
+WIDTHS = (16, 32, 64, 32, 16)
+NFEAT = 7
+GAIN = 10.0  # "error" targets: network output = GAIN x (normalised true model - current)
+
+
+# ================================================================================ network
+class ConvLayer:
+    def __init__(self, cin, cout, relu, gen, device="cuda"):
+        import torch
+        std = math.sqrt((2.0 if relu else 1.0) / (27 * cin))
+        self.cin, self.cout, self.relu = cin, cout, relu
+        self.w = (torch.randn((27, cout, cin), generator=gen) * std).to(device)
+        self.b = torch.zeros(cout, device=device)
+        self.wb = self.wt = None
+
+    def prep(self):
+        self.wb, self.wt = conv3d.prep_weights(self.w)
+
+
+class PreconditionerNet:
+    """4 conv layers (16-64 channels) on the tcgen05 conv3d kernels, with Adam."""
+
+    def __init__(self, widths=WIDTHS, seed=0, device="cuda", target="error"):
+        import torch
+        gen = torch.Generator().manual_seed(seed)
+        self.target = target  # what the output predicts: "error" or "update" (see invert)
+        n = len(widths) - 1
+        self.layers = [ConvLayer(widths[i], widths[i + 1], i < n - 1, gen, device)
+                       for i in range(n)]
+        self.ws = conv3d.WgradWorkspace()
+        self._acts = None
+        self._adam = None
+        self.steps = 0
+        if device == "cuda":
+            self.prep()
+
+    def prep(self):
+        for L in self.layers:
+            L.prep()
+
+    def parameters(self):
+        out = []
+        for L in self.layers:
+            out += [L.w, L.b]
+        return out
+
+    def forward(self, x, keep=False):
+        """x: (ny, nz, nx, 16) BF16 -> (ny, nz, nx, 16) FP32."""
+        acts = [x]
+        h = x
+        for i, L in enumerate(self.layers):
+            last = i == len(self.layers) - 1
+            yb, yf = conv3d.forward(h, L.wb, L.b, relu=L.relu, out_bf16=not last, out_f32=last)
+            h = yf if last else yb
+            acts.append(h)
+        if keep:
+            self._acts = acts
+        return h
+
+    def backward(self, dy):
+        """dy: dLoss/dOutput (ny, nz, nx, 16) FP32 -> [(dw, db)] per layer (needs forward(keep=True))."""
+        import torch
+        acts = self._acts
+        g = dy.to(torch.bfloat16).contiguous()
+        grads = [None] * len(self.layers)
+        for i in reversed(range(len(self.layers))):
+            L = self.layers[i]
+            grads[i] = conv3d.backward_weights(acts[i], g, self.ws)
+            if i > 0:
+                # input of layer i = ReLU output of layer i-1: its mask gates the data gradient
+                g = conv3d.backward_data(g, L.wt, L.cin, relu_mask=acts[i])
+        return grads
+
+    def adam_step(self, grads, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        import torch
+        params = self.parameters()
+        flat = []
+        for dw, db in grads:
+            flat += [dw, db]
+        if self._adam is None:
+            self._adam = [(torch.zeros_like(p), torch.zeros_like(p)) for p in params]
+        self.steps += 1
+        c1 = 1.0 - beta1 ** self.steps
+        c2 = 1.0 - beta2 ** self.steps
+        for p, g, (m, v) in zip(params, flat, self._adam):
+            m.mul_(beta1).add_(g, alpha=1.0 - beta1)
+            v.mul_(beta2).addcmul_(g, g, value=1.0 - beta2)
+            p.addcdiv_(m / c1, (v / c2).sqrt_().add_(eps), value=-lr)
+        if params[0].is_cuda:
+            self.prep()
+
+    def state_dict(self):
+        return {f"w{i}": L.w.detach().cpu().numpy() for i, L in enumerate(self.layers)} | \
+               {f"b{i}": L.b.detach().cpu().numpy() for i, L in enumerate(self.layers)}
+
+    def load_state_dict(self, sd):
+        import torch
+        for i, L in enumerate(self.layers):
+            L.w = torch.as_tensor(sd[f"w{i}"]).to(L.w.device)
+            L.b = torch.as_tensor(sd[f"b{i}"]).to(L.b.device)
+        if self.layers[0].w.is_cuda:
+            self.prep()
+
+
+def features(g3, p3):
+    """(3, ny, nz, nx) gradient and normalised model -> (ny, nz, nx, 16) BF16 features."""
+    import torch
+    _, ny, nz, nx = g3.shape
+    f = torch.zeros((ny, nz, nx, WIDTHS[0]), dtype=torch.float32, device=g3.device)
+    for c in range(3):
+        s = g3[c].abs().max().clamp_min(1e-30)
+        f[..., c] = g3[c] / s
+        f[..., 3 + c] = p3[c] - 1.0
+    f[..., 6] = (torch.arange(nz, device=g3.device, dtype=torch.float32) / nz)[None, :, None]
+    return f.to(torch.bfloat16).contiguous()
+
+
+def mse_grad(out, target):
+    """Loss and dLoss/dout for the mean squared error over channels 0-2."""
+    import torch
+    d = torch.zeros_like(out)
+    diff = out[..., :3] - target
+    n = diff.numel()
+    d[..., :3] = diff * (2.0 / n)
+    return float((diff * diff).sum() / n), d
+
+
+def train(net, samples, epochs=30, lr=2e-3, seed=0, log=None):
+    """samples: list of (features BF16 volume, target (ny, nz, nx, 3) FP32).  Returns the
+    mean loss of each epoch."""
+    rng = np.random.default_rng(seed)
+    hist = []
+    for ep in range(epochs):
+        tot = 0.0
+        for k in rng.permutation(len(samples)):
+            x, t = samples[k]
+            out = net.forward(x, keep=True)
+            loss, d = mse_grad(out, t)
+            net.adam_step(net.backward(d), lr=lr)
+            tot += loss
+        hist.append(tot / max(1, len(samples)))
+        if log:
+            log(f"epoch {ep}: loss {hist[-1]:.5f}")
+    conv3d.status()
+    return hist
+
+
+# ============================================================================= inversion
+@dataclasses.dataclass
+class ProblemSpec:
+    nx: int = 48
+    ny: int = 48
+    nz: int = 40
+    dx: float = 10.0
+    lenpml: int = 8
+    fq: float = 12.0
+    nt: int = 320
+    nshots: int = 4
+    nrec: int = 8
+    seed: int = 0
+    smooth_m: float = 150.0
+
+
+class InversionProblem:
+    """Seeded true / initial model, earthquake-style MT sources at depth and surface
+    receivers; misfit and exact gradient evaluations through one ShotBatch."""
+
+    def __init__(self, spec: ProblemSpec):
+        import torch
+        from . import configs
+        from .engine import ShotBatch
+        s = self.spec = spec
+        rng = np.random.default_rng(spec.seed)
+        vp, vs, rho = configs.layered_anomaly_model(s.ny, s.nz, s.nx, s.dx, spec.seed,
+                                                    n_layers=4, n_anomalies=3, sigma_m=60.0,
+                                                    vpvs=1.8)
+        vp0, vs0, rho0 = configs.smooth_model(vp, vs, rho, s.smooth_m / s.dx)
+        self.dt = configs.cfl_dt(s.dx, float(max(vp.max(), vp0.max())))
+        self.w = torch.as_tensor(configs.ricker(s.fq, self.dt, s.nt)).cuda()
+        self.cp = configs.cpml_profiles(s.fq, self.dt, s.dx, s.lenpml, float(max(vp.max(), vp0.max())),
+                                        s.nx, s.ny, s.nz)
+        rx, ry, rz = configs.surface_receivers(s.nx, s.ny, s.lenpml, s.nrec, s.nrec)
+        self.rec = np.stack([rx, ry, rz], axis=1)
+        lo = s.lenpml + 4
+        self.srcs = []
+        for _ in range(s.nshots):
+            self.srcs.append(([int(rng.integers(lo, s.nx - lo)), int(rng.integers(lo, s.ny - lo)),
+                               int(rng.integers(s.nz // 2, s.nz - lo))],
+                              configs.random_moment_tensor(rng)))
+        dev = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).cuda()  # noqa: E731
+        self.true = torch.stack([dev(vp), dev(vs), dev(rho)])
+        self.init = torch.stack([dev(vp0), dev(vs0), dev(rho0)])
+        self.scale = self.init.mean(dim=(1, 2, 3)).reshape(3, 1, 1, 1)
+        self.batch = ShotBatch()
+        lam, mu = self._lame(self.true)
+        for src, mt in self.srcs:
+            self.batch.add(nx=s.nx, ny=s.ny, nz=s.nz, lenpml=s.lenpml, dx=s.dx, dt=self.dt,
+                           nt=s.nt, cpml=self.cp, lam=lam, mu=mu, rho=self.true[2], wavelet=self.w,
+                           src=[src], mt=[mt], rec=self.rec)
+        self.obs = self.batch.forward().clone()
+        self.solves = 0
+
+    @staticmethod
+    def _lame(m):
+        vp, vs, rho = m[0], m[1], m[2]
+        mu = (vs * vs * rho).contiguous()
+        lam = (vp * vp * rho - 2.0 * mu).contiguous()
+        return lam, mu
+
+    def _set(self, m):
+        lam, mu = self._lame(m)
+        rho = m[2].contiguous()
+        for i in range(len(self.srcs)):
+            self.batch.set_model(i, lam, mu, rho)
+
+    def misfit(self, p):
+        """Misfit of the normalised model p (one forward solve)."""
+        self._set(p * self.scale)
+        mod = self.batch.forward()
+        _, mis = self.batch.residual_misfit(mod, self.obs)
+        self.solves += 1
+        return float(mis.sum())
+
+    def gradient(self, p):
+        """(misfit, dJ/dp) for the normalised model p (forward + adjoint solve); the exact
+        gradient, smoothed (sigma 1 cell) and masked at the absorbing frame like the
+        reference's post-processing."""
+        import torch
+        from .engine import chain_rule, smooth_mask
+        m = p * self.scale
+        self._set(m)
+        mod = self.batch.forward(checkpoints=True)
+        res, mis = self.batch.residual_misfit(mod, self.obs)
+        g, _ = self.batch.gradient(res, exact=True)
+        self.solves += 2
+        s = self.spec
+        n = s.nx * s.ny * s.nz
+        gv = g.reshape(len(self.srcs), 3, s.ny, s.nz, s.nx).sum(dim=0).contiguous()
+        gl, gm, gr = gv[0].contiguous(), gv[1].contiguous(), gv[2].contiguous()
+        chain_rule(gl, gm, gr, m[0].contiguous(), m[1].contiguous(), m[2].contiguous())
+        out = torch.stack([gl, gm, gr])
+        tmp = torch.empty_like(out[0])
+        for c in range(3):
+            smooth_mask(out[c], 1.0, s.lenpml, 2, tmp)
+        out *= self.scale  # dJ/dp = dJ/dm * scale
+        assert out.numel() == 3 * n
+        return float(mis.sum()), out
+
+    def model_error(self, p):
+        return float(((p * self.scale - self.true) / self.true).pow(2).mean().sqrt())
+
+
+class LBFGS:
+    """Standard L-BFGS two-loop recursion on the normalised model (float64 dots, memory m)."""
+
+    def __init__(self, m=5):
+        self.m = m
+        self.s, self.y = [], []
+
+    def update(self, s, y):
+        import torch
+        sy = float(torch.sum(s.double() * y.double()))
+        if sy <= 1e-30:
+            return
+        self.s.append(s)
+        self.y.append(y)
+        if len(self.s) > self.m:
+            self.s.pop(0)
+            self.y.pop(0)
+
+    def direction(self, g):
+        import torch
+        q = g.clone()
+        al = []
+        for s, y in zip(reversed(self.s), reversed(self.y)):
+            rho = 1.0 / float(torch.sum(y.double() * s.double()))
+            a = rho * float(torch.sum(s.double() * q.double()))
+            q -= a * y
+            al.append((a, rho, s, y))
+        if self.s:
+            s, y = self.s[-1], self.y[-1]
+            q *= float(torch.sum(s.double() * y.double()) / torch.sum(y.double() * y.double()))
+        for a, rho, s, y in reversed(al):
+            b = rho * float(torch.sum(y.double() * q.double()))
+            q += (a - b) * s
+        return -q
+
+
+def _line_search(prob, p, J, g, d, alpha0, tries=6, c1=1e-4):
+    """Armijo backtracking; returns (alpha, J_new) or (None, J)."""
+    import torch
+    gd = float(torch.sum(g.double() * d.double()))
+    if not gd < 0:
+        return None, J
+    a = alpha0
+    for _ in range(tries):
+        Jn = prob.misfit(p + a * d)
+        if math.isfinite(Jn) and Jn <= J + c1 * a * gd:
+            return a, Jn
+        a *= 0.5
+    return None, J
+
+
+def invert(prob, iters, net=None, first_step=0.02, record=None, target="error", log=None,
+           learned_iters=None, learned_tries=2):
+    """Plain (net=None) or learned-direction inversion.  Returns a history of dicts
+    (iteration, solves so far, misfit, model error, direction used).
+
+    `record`, when a list, receives one training pair per iteration: the features and, for
+    target "error", GAIN x (true model - current model) in normalised units (the update a
+    perfect preconditioner would take; the seeded problems know their true model), or, for
+    target "update", the accepted L-BFGS update scaled to unit maximum.  A network trained
+    on "error" targets proposes its output / GAIN with a unit first trial step; one trained
+    on "update" targets is scaled to the length of the previous accepted step.
+
+    learned_iters: use the network only in the first that many iterations (None: always);
+    learned_tries: line-search trials a learned direction gets before the iteration falls
+    back to L-BFGS."""
+    import torch
+    p = (prob.init / prob.scale).contiguous()
+    lb = LBFGS(5)
+    prob.solves = 0
+    J, g = prob.gradient(p)
+    hist = [dict(it=0, solves=prob.solves, misfit=J, model_error=prob.model_error(p), used="init")]
+    last_step = first_step
+    for it in range(1, iters + 1):
+        used = None
+        step = None
+        if net is not None and (learned_iters is None or it <= learned_iters):
+            out = net.forward(features(g, p))
+            d = out[..., :3].permute(3, 0, 1, 2).contiguous()
+            dmax = float(d.abs().max())
+            if net.target == "error":
+                d /= GAIN
+                a0 = 1.0
+            else:
+                a0 = last_step / max(dmax, 1e-30)
+            if dmax > 0:
+                a, Jn = _line_search(prob, p, J, g, d, a0, tries=learned_tries)
+                if a is not None:
+                    step, used = a * d, "learned"
+        if step is None:
+            d = lb.direction(g)
+            a0 = 1.0 if lb.s else first_step / max(float(d.abs().max()), 1e-30)
+            a, Jn = _line_search(prob, p, J, g, d, a0)
+            if a is None:
+                hist.append(dict(it=it, solves=prob.solves, misfit=J,
+                                 model_error=prob.model_error(p), used="stalled"))
+                break
+            step, used = a * d, ("fallback" if net is not None and (
+                learned_iters is None or it <= learned_iters) else "lbfgs")
+        if record is not None:
+            t = ((prob.true / prob.scale - p) * GAIN if target == "error"
+                 else step / step.abs().max())
+            record.append((features(g, p), t.permute(1, 2, 3, 0).contiguous()))
+        p_new = p + step
+        J_new, g_new = prob.gradient(p_new)
+        lb.update(step, g_new - g)
+        last_step = float(step.abs().max())
+        p, J, g = p_new, J_new, g_new
+        hist.append(dict(it=it, solves=prob.solves, misfit=J, model_error=prob.model_error(p),
+                         used=used))
+        if log:
+            log(f"it {it}: J {J:.4e} solves {prob.solves} ({used})")
+    return hist
+
+
+def solves_to_reach(hist, target):
+    for h in hist:
+        if h["misfit"] <= target:
+            return h["solves"]
+    return None
+
+
+POLICIES = {"always": dict(learned_iters=None), "first2": dict(learned_iters=2),
+            "first4": dict(learned_iters=4)}
+
+
+def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=12, epochs=40,
+               spec=None, target="error", log=None):
+    """Train on plain-L-BFGS runs of seeded models, then, on unseen seeds, compare plain
+    L-BFGS with each learned policy: the solves each needs to reach plain L-BFGS's final
+    misfit (None: not reached within `iters` iterations)."""
+    import time
+    base = spec or ProblemSpec()
+    samples = []
+    t0 = time.time()
+    for s in train_seeds:
+        prob = InversionProblem(dataclasses.replace(base, seed=s))
+        invert(prob, iters, record=samples, target=target)
+        prob.batch.close()
+    t_data = time.time() - t0
+    net = PreconditionerNet(seed=0, target=target)
+    t0 = time.time()
+    losses = train(net, samples, epochs=epochs, log=log)
+    t_train = time.time() - t0
+    tests = []
+    for ts in test_seeds:
+        prob = InversionProblem(dataclasses.replace(base, seed=ts))
+        plain = invert(prob, iters, log=log)
+        target_j = plain[-1]["misfit"]
+        row = dict(seed=ts, target_misfit=target_j, solves_plain=plain[-1]["solves"],
+                   plain=plain, policies={})
+        for name, kw in POLICIES.items():
+            h = invert(prob, iters, net=net, log=log, **kw)
+            row["policies"][name] = dict(solves=solves_to_reach(h, target_j),
+                                         final_misfit=h[-1]["misfit"],
+                                         fallbacks=sum(x["used"] == "fallback" for x in h),
+                                         history=h)
+        prob.batch.close()
+        tests.append(row)
+    summary = {}
+    for name in POLICIES:
+        r = [t["solves_plain"] / t["policies"][name]["solves"] if t["policies"][name]["solves"]
+             else 0.0 for t in tests]
+        summary[name] = dict(solve_ratio_per_seed=r, reached=sum(x > 0 for x in r))
+    return dict(spec=dataclasses.asdict(base), target=target, train_seeds=list(train_seeds),
+                test_seeds=list(test_seeds), iters=iters, epochs=epochs, n_samples=len(samples),
+                loss_first=losses[0], loss_last=losses[-1], data_s=t_data, train_s=t_train,
+                summary=summary, tests=tests)
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="learned-preconditioner experiment")
+    ap.add_argument("--iters", type=int, default=12)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--train", type=int, default=8, help="number of training seeds")
+    ap.add_argument("--target", default="error", choices=["error", "update"])
+    ap.add_argument("--test-seeds", default="7,8,9")
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    r = experiment(train_seeds=tuple(range(100, 100 + a.train)),
+                   test_seeds=tuple(int(v) for v in a.test_seeds.split(",")),
+                   iters=a.iters, epochs=a.epochs, target=a.target, log=print)
+    s = json.dumps(r, indent=1)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(s)
+    print(json.dumps({k: v for k, v in r.items() if k != "tests"}))

@@ -149,8 +149,15 @@ def bench(shape=(128, 128, 256), pairs=((16, 32), (32, 64), (64, 32), (32, 16)),
 
 
 if __name__ == "__main__":
+    import argparse
     import json
-    import sys
-    shp = tuple(int(v) for v in sys.argv[1].split(",")) if len(sys.argv) > 1 else (128, 128, 256)
-    for r in bench(shp):
+    ap = argparse.ArgumentParser(description="conv3d kernel throughput")
+    ap.add_argument("shape", nargs="?", default="128,128,256", help="ny,nz,nx")
+    ap.add_argument("--pairs", default="16x32,32x64,64x32,32x16", help="cin x cout list")
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=2)
+    a = ap.parse_args()
+    shp = tuple(int(v) for v in a.shape.split(","))
+    prs = tuple(tuple(int(v) for v in p.split("x")) for p in a.pairs.split(","))
+    for r in bench(shp, prs, reps=a.reps, warmup=a.warmup):
         print(json.dumps(r))

@@ -9,21 +9,23 @@
 // x + kw - 1).
 //
 // forward / data gradient  (efm_conv_fwd_kernel)
-//   GEMM: M = 128 voxels along x, N = cout, K = 27 cin.  All 27 weight taps stay resident
-//   in shared memory (loaded by TMA once per block).  The block walks its tiles; for each
-//   tile the nine (kd, kh) input rows arrive by TMA as K-major slabs of 136 rows (x0-4 ..
-//   x0+131) x 8 channels, and the three kw taps read the same slab at start addresses 3, 4,
-//   5 rows in.  Warp 0 issues TMA, warp 1 issues tcgen05.mma into a double-buffered TMEM
-//   accumulator, warps 2-5 drain TMEM (tcgen05.ld) and apply bias + ReLU (forward) or the
-//   ReLU mask of the layer below (data gradient) while the next tile accumulates.
+//   GEMM: M = 128 voxels along x, N = cout, K = 27 cin, for 4 consecutive z rows at once.
+//   All 27 weight taps stay resident in shared memory (loaded by TMA once per block).  The
+//   block walks its tiles (128 x-voxels x 4 z-rows of one y plane); the 18 input rows
+//   (kd, z0-1 .. z0+4) a tile reads arrive by TMA as K-major slabs of 136 rows (x0-4 ..
+//   x0+131) x 8 channels, each slab feeding every output row within reach, and the three
+//   kw taps read the same slab at start addresses 3, 4, 5 rows in.  Warp 0 issues TMA,
+//   warp 1 issues tcgen05.mma into double-buffered TMEM accumulators (4 rows x cout
+//   columns each), warps 2-5 drain TMEM (tcgen05.ld) and apply bias + ReLU (forward) or
+//   the ReLU mask of the layer below (data gradient) while the next tile accumulates.
 //   The data gradient is the forward kernel with cin/cout swapped and the taps mirrored
 //   (weights prepared by efm_conv_prep_kernel).
 //
 // weight gradient  (efm_conv_wgrad_kernel)
 //   GEMM: M = (kd, kh, ci) rows -- 128 / cin (kd, kh) pairs of cin channels per tile --,
 //   N = cout, K = voxels.  Both operands are MN-major slabs read straight from the
-//   channels-last volumes (8 channels x 64 or 72 voxels per TMA box); the three kw taps
-//   again come from start-address shifts of one 72-row input slab, accumulated in three
+//   channels-last volumes (8 channels x 128 or 136 voxels per TMA box); the three kw taps
+//   again come from start-address shifts of one 136-row input slab, accumulated in three
 //   TMEM column ranges.  Blocks split K; partial sums go to a workspace and a second kernel
 //   reduces them in a fixed order (deterministic).
 //
@@ -50,12 +52,13 @@ constexpr int CV_MT = 128;                 // voxels per forward tile (GEMM M)
 constexpr int CV_AROWS = 136;              // forward input slab rows: x0-4 .. x0+131
 constexpr int CV_ASLAB = CV_AROWS * 16;    // bytes of one 8-channel slab
 constexpr int CV_STAGES = 4;
+constexpr int CV_R = 4;                    // output z rows per forward tile
 constexpr int CV_THREADS = 192;            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int CV_MIN_SMEM = 116 * 1024;    // one block per SM: TMEM allocation never waits
-constexpr int WG_K = 64;                   // voxels per weight-gradient K chunk
-constexpr int WG_AROWS = 72;               // x0-4 .. x0+67
-constexpr int WG_ASLAB = WG_AROWS * 16;    // 1152
-constexpr int WG_BSLAB = WG_K * 16;        // 1024
+constexpr int WG_K = 128;                  // voxels per weight-gradient K chunk
+constexpr int WG_AROWS = 136;              // x0-4 .. x0+131
+constexpr int WG_ASLAB = WG_AROWS * 16;    // 2176
+constexpr int WG_BSLAB = WG_K * 16;        // 2048
 
 __device__ unsigned int g_conv_err;
 
@@ -134,6 +137,9 @@ __device__ __forceinline__ void store_bf16x8(__nv_bfloat16 *dst, const float *v)
 
 // ------------------------------------------------------------------ forward / data gradient
 // MODE 0: y = act(conv(x) + bias) (bf16 and/or fp32 out); MODE 1: y = conv(x) * [mask > 0].
+// A tile is CV_MT voxels along x times CV_R consecutive z rows (one accumulator each); the
+// 3 (CV_R + 2) input rows (kd, zi) it reads arrive one slab per stage and feed every output
+// row r with kh = zi - r in 0..2.
 template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(CV_THREADS, 1)
 efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_w,
@@ -144,15 +150,18 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
     constexpr int NG = CIN / 8;                       // 8-channel groups (K core matrices)
     constexpr int WBYTES = 27 * CIN * COUT * 2;
     constexpr int ASTAGE = NG * CV_ASLAB;
+    constexpr int R = CV_R;
+    constexpr int NSLAB = 3 * (R + 2);                // input rows per tile
     constexpr uint32_t IDESC = efm_idesc_bf16(CV_MT, COUT, false, false);
-    constexpr uint32_t NCOLS = COUT * 2 <= 32 ? 32 : COUT * 2;  // double-buffered accumulator
+    constexpr uint32_t NCOLS = 2 * R * COUT <= 32 ? 32 : 2 * R * COUT;  // double-buffered
+    static_assert(2 * R * COUT <= 512, "TMEM columns");
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ Sync S;
     unsigned char *wsm = smem;
     unsigned char *asm_ = smem + WBYTES;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int xt = (nx + CV_MT - 1) / CV_MT;
-    const int ntiles = xt * nz * ny;
+    const int xt = (nx + CV_MT - 1) / CV_MT, zt = (nz + R - 1) / R;
+    const int ntiles = xt * zt * ny;
     cv_setup(S, 128, NCOLS);
     volatile int *abort = &S.abort;
     bool mma_issued = false;
@@ -170,14 +179,15 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
         bool issued[CV_STAGES] = {};
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const int x0 = (tile % xt) * CV_MT, z = (tile / xt) % nz, y = tile / (xt * nz);
-            for (int kk = 0; kk < 9; ++kk) {
+            const int x0 = (tile % xt) * CV_MT, z0 = ((tile / xt) % zt) * R, y = tile / (xt * zt);
+            for (int k = 0; k < NSLAB; ++k) {
+                const int kd = k / (R + 2), zi = k % (R + 2);
                 if (!cv_wait(&S.empty[st], ph ^ 1u, abort)) { ok = false; break; }
                 efm_mbar_expect_tx(&S.full[st], ASTAGE);
                 unsigned char *dst = asm_ + st * ASTAGE;
                 for (int g = 0; g < NG; ++g)
                     efm_tma_load_4d(dst + g * CV_ASLAB, &tm_x, &S.full[st], 8 * g, x0 - 4,
-                                    z + kk % 3 - 1, y + kk / 3 - 1);
+                                    z0 + zi - 1, y + kd - 1);
                 issued[st] = true;
                 issued_parity[st] = ph;
                 if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
@@ -197,19 +207,27 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
             if (!cv_wait(&S.tempty[acc], aph ^ 1u, abort)) { ok = false; break; }
             efm_tc_fence_after();
-            const uint32_t d = S.tmem + acc * COUT;
-            for (int kk = 0; kk < 9 && ok; ++kk) {
+            uint32_t started = 0;  // bit r: accumulator of output row r holds a partial sum
+            for (int k = 0; k < NSLAB && ok; ++k) {
+                const int kd = k / (R + 2), zi = k % (R + 2);
                 if (!cv_wait(&S.full[st], ph, abort)) { ok = false; break; }
                 efm_tc_fence_after();
                 const uint32_t a0 = abase + st * ASTAGE;
 #pragma unroll
-                for (int kw = 0; kw < 3; ++kw) {
-                    const int t = kk * 3 + kw;
+                for (int r = 0; r < R; ++r) {
+                    const int kh = zi - r;
+                    if (kh < 0 || kh > 2) continue;
+                    const uint32_t d = S.tmem + (acc * R + r) * COUT;
 #pragma unroll
-                    for (int j = 0; j < CIN / 16; ++j) {
-                        const uint64_t a = efm_sdesc(a0 + 2 * j * CV_ASLAB + (kw + 3) * 16, CV_ASLAB, 128);
-                        const uint64_t b = efm_sdesc(wbase + (2 * j * 27 + t) * COUT * 16, 27 * COUT * 16, 128);
-                        efm_mma_bf16(d, a, b, IDESC, (kk | kw | j) != 0);
+                    for (int kw = 0; kw < 3; ++kw) {
+                        const int t = kd * 9 + kh * 3 + kw;
+#pragma unroll
+                        for (int j = 0; j < CIN / 16; ++j) {
+                            const uint64_t a = efm_sdesc(a0 + 2 * j * CV_ASLAB + (kw + 3) * 16, CV_ASLAB, 128);
+                            const uint64_t b = efm_sdesc(wbase + (2 * j * 27 + t) * COUT * 16, 27 * COUT * 16, 128);
+                            efm_mma_bf16(d, a, b, IDESC, (started >> r) & 1u);
+                            started |= 1u << r;
+                        }
                     }
                 }
                 mma_issued = true;
@@ -221,7 +239,7 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
             if (++acc == 2) { acc = 0; aph ^= 1u; }
         }
     } else if (warp >= 2) {
-        // ---------------- epilogue: TMEM -> registers -> global
+        // ---------------- epilogue: TMEM -> registers -> global, one output row at a time
         const int q = warp % 4;           // TMEM lane quadrant this warp may read
         const int row = q * 32 + lane;    // voxel of the tile
         int acc = 0;
@@ -229,43 +247,46 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             if (!cv_wait(&S.tfull[acc], aph, abort)) break;
             efm_tc_fence_after();
-            float v[COUT];
+            const int x0 = (tile % xt) * CV_MT, z0 = ((tile / xt) % zt) * R, y = tile / (xt * zt);
+            const int x = x0 + row;
+            for (int r = 0; r < R; ++r) {
+                float v[COUT];
 #pragma unroll
-            for (int c = 0; c < COUT; c += 16)
-                efm_tmem_ld16(S.tmem + ((uint32_t)(q * 32) << 16) + acc * COUT + c, v + c);
+                for (int c = 0; c < COUT; c += 16)
+                    efm_tmem_ld16(S.tmem + ((uint32_t)(q * 32) << 16) + (acc * R + r) * COUT + c, v + c);
+                const int z = z0 + r;
+                if (x >= nx || z >= nz) continue;
+                const int64_t vox = ((int64_t)y * nz + z) * nx + x;
+                if (MODE == 0) {
+#pragma unroll
+                    for (int c = 0; c < COUT; ++c) {
+                        float u = v[c] + (bias ? bias[c] : 0.f);
+                        v[c] = (relu && u < 0.f) ? 0.f : u;
+                    }
+                    if (y_f32) {
+                        float4 *o = reinterpret_cast<float4 *>(y_f32 + vox * COUT);
+#pragma unroll
+                        for (int c = 0; c < COUT; c += 4) o[c / 4] = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                    }
+                } else if (mask != nullptr) {
+                    const uint4 *m = reinterpret_cast<const uint4 *>(mask + vox * COUT);
+#pragma unroll
+                    for (int c = 0; c < COUT; c += 8) {
+                        const uint4 u = m[c / 8];
+                        const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&u);
+#pragma unroll
+                        for (int i = 0; i < 8; ++i)
+                            if (!(__bfloat162float(h[i]) > 0.f)) v[c + i] = 0.f;
+                    }
+                }
+                if (y_bf16) {
+#pragma unroll
+                    for (int c = 0; c < COUT; c += 8) store_bf16x8(y_bf16 + vox * COUT + c, v + c);
+                }
+            }
             efm_tc_fence_before();
             efm_mbar_arrive(&S.tempty[acc]);
             if (++acc == 2) { acc = 0; aph ^= 1u; }
-            const int x0 = (tile % xt) * CV_MT, z = (tile / xt) % nz, y = tile / (xt * nz);
-            const int x = x0 + row;
-            if (x >= nx) continue;
-            const int64_t vox = ((int64_t)y * nz + z) * nx + x;
-            if (MODE == 0) {
-#pragma unroll
-                for (int c = 0; c < COUT; ++c) {
-                    float r = v[c] + (bias ? bias[c] : 0.f);
-                    v[c] = (relu && r < 0.f) ? 0.f : r;
-                }
-                if (y_f32) {
-                    float4 *o = reinterpret_cast<float4 *>(y_f32 + vox * COUT);
-#pragma unroll
-                    for (int c = 0; c < COUT; c += 4) o[c / 4] = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
-                }
-            } else if (mask != nullptr) {
-                const uint4 *m = reinterpret_cast<const uint4 *>(mask + vox * COUT);
-#pragma unroll
-                for (int c = 0; c < COUT; c += 8) {
-                    const uint4 u = m[c / 8];
-                    const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&u);
-#pragma unroll
-                    for (int i = 0; i < 8; ++i)
-                        if (!(__bfloat162float(h[i]) > 0.f)) v[c + i] = 0.f;
-                }
-            }
-            if (y_bf16) {
-#pragma unroll
-                for (int c = 0; c < COUT; c += 8) store_bf16x8(y_bf16 + vox * COUT + c, v + c);
-            }
         }
     }
     __syncwarp();
@@ -512,7 +533,7 @@ int launch_fwd(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap 
     auto k = efm_conv_fwd_kernel<CIN, COUT, MODE>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
-    const int64_t tiles = (int64_t)((d->nx + CV_MT - 1) / CV_MT) * d->nz * d->ny;
+    const int64_t tiles = (int64_t)((d->nx + CV_MT - 1) / CV_MT) * ((d->nz + CV_R - 1) / CV_R) * d->ny;
     const int grid = (int)(tiles < num_sms() ? tiles : num_sms());
     k<<<grid, CV_THREADS, smem, s>>>(tx, tw, d->nx, d->ny, d->nz, bias, relu,
                                       static_cast<const __nv_bfloat16 *>(mask),
@@ -536,7 +557,7 @@ int dispatch_fwd(int cin, int cout, const efm_conv_desc *d, const CUtensorMap &t
 
 int wgrad_splits(const efm_conv_desc *d, int nq) {
     const int64_t units = (int64_t)((d->nx + WG_K - 1) / WG_K) * d->nz * d->ny;
-    int64_t s = (num_sms() + nq - 1) / nq;
+    int64_t s = num_sms() / nq;  // one wave of single-block SMs
     if (s > units) s = units;
     return (int)(s < 1 ? 1 : s);
 }

@@ -378,6 +378,11 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="error", 
             d = lb.direction(g)
             a0 = 1.0 if lb.s else first_step / max(float(d.abs().max()), 1e-30)
             a, Jn = _line_search(prob, p, J, g, d, a0)
+            if a is None and lb.s:
+                # restart: drop the curvature pairs, retry along the steepest descent
+                lb = LBFGS(lb.m)
+                d = -g
+                a, Jn = _line_search(prob, p, J, g, d, first_step / max(float(d.abs().max()), 1e-30))
             if a is None:
                 hist.append(dict(it=it, solves=prob.solves, misfit=J,
                                  model_error=prob.model_error(p), used="stalled"))

@@ -14,7 +14,7 @@ import pytest
 from conftest import rel_err
 
 PAIRS = [(16, 32), (32, 64), (64, 32), (32, 16), (16, 16), (64, 16)]
-GRIDS = [(6, 5, 24), (3, 4, 136)]
+GRIDS = [(6, 5, 24), (3, 4, 136), (2, 9, 40)]
 
 
 def _ref_conv(x, w, b, relu):

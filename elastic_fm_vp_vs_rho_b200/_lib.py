@@ -97,6 +97,7 @@ SIGNATURES = {
     "efm_lbfgs_direction": (_I, [_P, _P, _P, _P, _P, _I, _L, _I, _P]),
     "efm_smooth_mask": (_I, [_P, _P, _I, _I, _I, _F, _I, _I, _P]),
     "efm_chain_rule": (_I, [_P, _P, _P, _P, _P, _P, _L, _P]),
+    "efm_xcorr_residual_misfit": (_I, [_P, _P, _P, _P, _I, _I, _P, _P]),
     "efm_conv3d_supported": (_I, [_I, _I]),
     "efm_conv3d_prep_weights": (_I, [_I, _I, _P, _P, _P, _P]),
     "efm_conv3d_forward": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _I, _P, _P, _P]),

@@ -193,6 +193,26 @@ class ShotBatch:
                                           ptr(mis), stream_ptr(stream)))
         return res, mis
 
+    def residual_misfit_xcorr(self, mod, obs, res=None, stream=None):
+        """Cross-correlation adjoint source and misfit per instance (float64 tensor), the
+        reference's computeResidualCrossCorrelation / computeCostFunctionCrossCorrelation."""
+        import torch
+        if res is None:
+            res = torch.empty_like(mod)
+        mis = torch.empty(len(self.infos), dtype=torch.float64, device=mod.device)
+        obs = obs.contiguous()
+        work = torch.empty(9 * max(inf.nrec for inf in self.infos), dtype=torch.float64,
+                           device=mod.device)
+        for i, inf in enumerate(self.infos):
+            o = inf.gather_off
+            n = 3 * inf.nt * inf.nrec
+            check(self._L.efm_xcorr_residual_misfit(
+                ctypes.c_void_p(mod.data_ptr() + 4 * o), ctypes.c_void_p(obs.data_ptr() + 4 * o),
+                ctypes.c_void_p(res.data_ptr() + 4 * o), ctypes.c_void_p(mis.data_ptr() + 8 * i),
+                inf.nt, inf.nrec, ptr(work), stream_ptr(stream)))
+            assert o + n <= mod.numel()
+        return res, mis
+
     def gradient(self, res, model=True, mt=False, nt_minus_1=False, exact=False, stream=None):
         """Adjoint pass.  Returns (grad buffer or None, mt grads (ninst, 4, 6) float64 or None).
 

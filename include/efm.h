@@ -264,6 +264,18 @@ EFM_API int efm_smooth_mask(float *g_dev, float *tmp_dev, int nx, int ny, int nz
 EFM_API int efm_chain_rule(float *g_lam_dev, float *g_mu_dev, float *g_rho_dev, const float *vp_dev,
                    const float *vs_dev, const float *rho_dev, int64_t n, void *stream);
 
+/*
+ * Normalised cross-correlation misfit of one instance's [3][nt][nrec] gathers
+ * (Elastic3D.computeResidualCrossCorrelation / computeCostFunctionCrossCorrelation,
+ * mainPropElastic3D_MT.py:2145-2209): res = m * (<m,o> / (|o| |m|^3) - o / (|m| |o|)) per
+ * trace, bracketed as the reference writes it (the adjoint source it injects)
+ * and *cost_dev (gather-wide normalisation, summed over the 3 components), with the
+ * reference's zero-norm / zero-product guards.  work_dev: 9 nrec doubles.
+ */
+EFM_API int efm_xcorr_residual_misfit(const float *mod_dev, const float *obs_dev, float *res_dev,
+                                      double *cost_dev, int nt, int nrec, double *work_dev,
+                                      void *stream);
+
 /* ------------------------------------------------ learned preconditioner: 3x3x3 conv3d
  *
  * No counterpart in the reference (which preconditions with gaussian_filter and L-BFGS,

@@ -317,6 +317,31 @@ def misfit(mod, obs):
     return res, 0.5 * float(np.sum(res * res))
 
 
+def xcorr_misfit(mod, obs):
+    """computeResidualCrossCorrelation + computeCostFunctionCrossCorrelation (:2145-2209)
+    on [3][nt][nrec] gathers, float64: per-trace adjoint source as the reference writes it
+    (:2179-2181), r = m * (<m,o> / (|o| |m|^3) - o / (|m| |o|)) -- the whole bracket times
+    the modelled trace -- (zero norms and zero products count as 1) and
+    the gather-wide cost sum_c 1 - <m_c,o_c> / (|m_c| |o_c|) (zero norms count as 1)."""
+    m = np.asarray(mod, np.float64)
+    o = np.asarray(obs, np.float64)
+    lm = np.sqrt(np.sum(m * m, axis=1, keepdims=True))
+    lo = np.sqrt(np.sum(o * o, axis=1, keepdims=True))
+    mo = np.sum(m * o, axis=1, keepdims=True)
+    lm = np.where(lm == 0, 1.0, lm)
+    lo = np.where(lo == 0, 1.0, lo)
+    mo = np.where(mo == 0, 1.0, mo)
+    res = m * (mo / (lo * lm ** 3) - o / (lm * lo))
+    cost = 0.0
+    for c in range(3):
+        a = np.sqrt(np.sum(m[c] * m[c]))
+        b = np.sqrt(np.sum(o[c] * o[c]))
+        a = 1.0 if a == 0 else a
+        b = 1.0 if b == 0 else b
+        cost += 1.0 - np.sum(m[c] * o[c]) / (a * b)
+    return res, float(cost)
+
+
 def _mt_strain(md: Model, bst: State, src):
     """kernel_Gradients_Mij (:337-372) without the wavelet factor: compliance-form
     strain of the adjoint stress at the source cell."""

@@ -10,7 +10,8 @@ Compute runs in ``libefm.so`` (hand-written CUDA, C ABI in ``include/efm.h``); t
 no CPU fallback.
 """
 from .elastic3d import (CPML, Alpha, Earthquake, Elastic3D, Gather, Geometry, Gradients,  # noqa: F401
-                        Model, Station, StressTensor, Wavelet)
+                        Model, Station, StressTensor, Wavelet, multifrequency_fwi,
+                        observed_data)
 from .engine import ShotBatch, chain_rule, dot, smooth_mask  # noqa: F401
 from .lbfgs import L_BFGS, compute_sk_yk  # noqa: F401
 from ._lib import EfmError  # noqa: F401

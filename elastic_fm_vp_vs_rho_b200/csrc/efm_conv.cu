@@ -51,7 +51,9 @@ namespace {
 constexpr int CV_MT = 128;                 // voxels per forward tile (GEMM M)
 constexpr int CV_AROWS = 136;              // forward input slab rows: x0-4 .. x0+131
 constexpr int CV_ASLAB = CV_AROWS * 16;    // bytes of one 8-channel slab
-constexpr int CV_STAGES = 4;
+constexpr int CV_STAGES = 4;               // weight-gradient ring depth
+constexpr int CV_MAX_STAGES = 8;
+constexpr int CV_SMEM_BUDGET = 200 * 1024; // forward ring: as deep as fits next to the weights
 constexpr int CV_R = 4;                    // output z rows per forward tile
 constexpr int CV_THREADS = 192;            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int CV_MIN_SMEM = 116 * 1024;    // one block per SM: TMEM allocation never waits
@@ -62,8 +64,15 @@ constexpr int WG_BSLAB = WG_K * 16;        // 2048
 
 __device__ unsigned int g_conv_err;
 
+// forward ring depth for a weight block of wbytes and input stages of astage bytes
+__host__ __device__ constexpr int cv_fwd_stages(int wbytes, int astage) {
+    return (CV_SMEM_BUDGET - wbytes) / astage > CV_MAX_STAGES ? CV_MAX_STAGES
+           : (CV_SMEM_BUDGET - wbytes) / astage < 2             ? 2
+                                                                 : (CV_SMEM_BUDGET - wbytes) / astage;
+}
+
 struct Sync {
-    uint64_t full[CV_STAGES], empty[CV_STAGES];
+    uint64_t full[CV_MAX_STAGES], empty[CV_MAX_STAGES];
     uint64_t wbar, tfull[2], tempty[2], drain;
     uint32_t tmem;
     int abort;
@@ -87,10 +96,10 @@ __device__ __forceinline__ void cv_drain_wait(uint64_t *bar, uint32_t parity) {
 }
 
 // Block set-up common to both kernels: barriers, TMEM allocation (warp 1).
-__device__ __forceinline__ void cv_setup(Sync &S, int epi_count, uint32_t ncols) {
+__device__ __forceinline__ void cv_setup(Sync &S, int epi_count, uint32_t ncols, int nstages) {
     const int warp = threadIdx.x / 32;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < CV_STAGES; ++s) {
+        for (int s = 0; s < nstages; ++s) {
             efm_mbar_init(&S.full[s], 1);
             efm_mbar_init(&S.empty[s], 1);
         }
@@ -152,6 +161,7 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
     constexpr int ASTAGE = NG * CV_ASLAB;
     constexpr int R = CV_R;
     constexpr int NSLAB = 3 * (R + 2);                // input rows per tile
+    constexpr int NST = cv_fwd_stages(WBYTES, ASTAGE);
     constexpr uint32_t IDESC = efm_idesc_bf16(CV_MT, COUT, false, false);
     constexpr uint32_t NCOLS = 2 * R * COUT <= 32 ? 32 : 2 * R * COUT;  // double-buffered
     static_assert(2 * R * COUT <= 512, "TMEM columns");
@@ -162,7 +172,7 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int xt = (nx + CV_MT - 1) / CV_MT, zt = (nz + R - 1) / R;
     const int ntiles = xt * zt * ny;
-    cv_setup(S, 128, NCOLS);
+    cv_setup(S, 128, NCOLS, NST);
     volatile int *abort = &S.abort;
     bool mma_issued = false;
 
@@ -175,8 +185,8 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
             efm_tma_load_3d(wsm + g * 27 * COUT * 16, &tm_w, &S.wbar, 8 * g, 0, 0);
         int st = 0;
         uint32_t ph = 0;
-        uint32_t issued_parity[CV_STAGES];
-        bool issued[CV_STAGES] = {};
+        uint32_t issued_parity[NST];
+        bool issued[NST] = {};
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
             const int x0 = (tile % xt) * CV_MT, z0 = ((tile / xt) % zt) * R, y = tile / (xt * zt);
@@ -190,18 +200,19 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
                                     z0 + zi - 1, y + kd - 1);
                 issued[st] = true;
                 issued_parity[st] = ph;
-                if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
+                if (++st == NST) { st = 0; ph ^= 1u; }
             }
         }
         if (!ok) {  // no load may still target this block's shared memory
-            for (int s = 0; s < CV_STAGES; ++s)
+            for (int s = 0; s < NST; ++s)
                 if (issued[s]) cv_drain_wait(&S.full[s], issued_parity[s]);
         }
         cv_drain_wait(&S.wbar, 0);
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer
         bool ok = cv_wait(&S.wbar, 0, abort);
-        const uint32_t wbase = efm_smem_addr(wsm), abase = efm_smem_addr(asm_);
+        const uint32_t abase = efm_smem_addr(asm_);
+        const uint64_t wdesc = efm_sdesc(efm_smem_addr(wsm), 27 * COUT * 16, 128);
         int st = 0, acc = 0;
         uint32_t ph = 0, aph = 0;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -212,19 +223,21 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
                 const int kd = k / (R + 2), zi = k % (R + 2);
                 if (!cv_wait(&S.full[st], ph, abort)) { ok = false; break; }
                 efm_tc_fence_after();
-                const uint32_t a0 = abase + st * ASTAGE;
+                // descriptors differ only in their start-address field: build one per stage
+                // / tap row and add the (compile-time) offsets >> 4 for kw and j
+                const uint64_t adesc = efm_sdesc(abase + st * ASTAGE, CV_ASLAB, 128);
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const int kh = zi - r;
                     if (kh < 0 || kh > 2) continue;
                     const uint32_t d = S.tmem + (acc * R + r) * COUT;
+                    const uint64_t bdesc = wdesc + (uint64_t)(((kd * 9 + kh * 3) * COUT * 16) >> 4);
 #pragma unroll
                     for (int kw = 0; kw < 3; ++kw) {
-                        const int t = kd * 9 + kh * 3 + kw;
 #pragma unroll
                         for (int j = 0; j < CIN / 16; ++j) {
-                            const uint64_t a = efm_sdesc(a0 + 2 * j * CV_ASLAB + (kw + 3) * 16, CV_ASLAB, 128);
-                            const uint64_t b = efm_sdesc(wbase + (2 * j * 27 + t) * COUT * 16, 27 * COUT * 16, 128);
+                            const uint64_t a = adesc + (uint64_t)((2 * j * CV_ASLAB + (kw + 3) * 16) >> 4);
+                            const uint64_t b = bdesc + (uint64_t)(((2 * j * 27 + kw) * COUT * 16) >> 4);
                             efm_mma_bf16(d, a, b, IDESC, (started >> r) & 1u);
                             started |= 1u << r;
                         }
@@ -232,7 +245,7 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
                 }
                 mma_issued = true;
                 efm_mma_commit(&S.empty[st]);  // frees the slab once these MMAs have read it
-                if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
+                if (++st == NST) { st = 0; ph ^= 1u; }
             }
             if (!ok) break;
             efm_mma_commit(&S.tfull[acc]);
@@ -313,7 +326,7 @@ efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_con
     const int xc = (nx + WG_K - 1) / WG_K;
     const int64_t units = (int64_t)xc * nz * ny;
     const int64_t u0 = units * split / nsplit, u1 = units * (split + 1) / nsplit;
-    cv_setup(S, 128, NCOLS);
+    cv_setup(S, 128, NCOLS, CV_STAGES);
     volatile int *abort = &S.abort;
     bool mma_issued = false;
 
@@ -356,12 +369,13 @@ efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_con
             if (!cv_wait(&S.full[st], ph, abort)) { ok = false; break; }
             efm_tc_fence_after();
             const uint32_t a0 = base + st * STAGE, b0 = a0 + ASTAGE;
+            const uint64_t adesc = efm_sdesc(a0, 128, WG_ASLAB), bdesc = efm_sdesc(b0, 128, WG_BSLAB);
 #pragma unroll
             for (int kw = 0; kw < 3; ++kw) {
 #pragma unroll
                 for (int j = 0; j < WG_K / 16; ++j) {
-                    const uint64_t a = efm_sdesc(a0 + 256 * j + (kw + 3) * 16, 128, WG_ASLAB);
-                    const uint64_t b = efm_sdesc(b0 + 256 * j, 128, WG_BSLAB);
+                    const uint64_t a = adesc + (uint64_t)((256 * j + (kw + 3) * 16) >> 4);
+                    const uint64_t b = bdesc + (uint64_t)((256 * j) >> 4);
                     efm_mma_bf16(S.tmem + kw * COUT, a, b, IDESC, (u != u0 || j != 0) ? 1u : 0u);
                 }
             }
@@ -528,7 +542,8 @@ int num_sms() {
 template <int CIN, int COUT, int MODE>
 int launch_fwd(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tw, const float *bias,
                int relu, const void *mask, void *yb, float *yf, cudaStream_t s) {
-    const int smem_need = 27 * CIN * COUT * 2 + CV_STAGES * (CIN / 8) * CV_ASLAB;
+    const int smem_need = 27 * CIN * COUT * 2 +
+                          cv_fwd_stages(27 * CIN * COUT * 2, (CIN / 8) * CV_ASLAB) * (CIN / 8) * CV_ASLAB;
     const int smem = smem_need > CV_MIN_SMEM ? smem_need : CV_MIN_SMEM;
     auto k = efm_conv_fwd_kernel<CIN, COUT, MODE>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

@@ -434,6 +434,24 @@ class Elastic3D:
         self.totalCostFunction = self._misfit
         self.costFunction.append(float(self.totalCostFunction))
 
+    def computeResidualCrossCorrelation(self):
+        """Cross-correlation adjoint source (:2145-2181) on the GPU
+        (efm_xcorr_residual_misfit): per trace r = m * (<m,o> / (|o| |m|^3) - o / (|m||o|))."""
+        mod = _dev(self.modGather.stack().reshape(-1))
+        obs = _dev(self.obsGather.stack().reshape(-1))
+        self._d_res, mis = self._eng.residual_misfit_xcorr(mod, obs)
+        self._xcorr_cost = float(mis[0].item())
+        r = self._d_res.view(3, self.nt, self.LenStations).cpu().numpy()
+        self.resGather.Vx, self.resGather.Vy, self.resGather.Vz = r[0].copy(), r[1].copy(), r[2].copy()
+
+    def computeCostFunctionCrossCorrelation(self, iter):
+        """sum over components of 1 - <m,o> / (|m| |o|) over the whole gather (:2183-2209);
+        after computeResidualCrossCorrelation."""
+        if not hasattr(self, "_xcorr_cost"):
+            self.computeResidualCrossCorrelation()
+        self.totalCostFunction = self._xcorr_cost
+        self.costFunction.append(float(self.totalCostFunction))
+
     def backwardFields_FowardFieldsRemake(self, saveFieldFlag=False):
         """Adjoint + reverse-time rebuild + imaging (:1929-2054).  mode 1 fills gk.Lambda,
         gk.Mu, gk.Rho; mode 0 fills the MT gradients over the same nt-1 steps."""
@@ -530,9 +548,14 @@ class Elastic3D:
         k = self.SrxIdx
         os.makedirs(os.path.join(d, "CostFunction"), exist_ok=True)
         os.makedirs(os.path.join(d, "TM"), exist_ok=True)
+        os.makedirs(os.path.join(d, "Gathers"), exist_ok=True)
         np.save(os.path.join(d, "CostFunction", f"costFunction{k}.npy"), self.costFunction)
         for c, v in hist.items():
             np.save(os.path.join(d, "TM", f"Mmod{c}{k}.npy"), v)
+        # :2330-2335
+        for comp in ("Vx", "Vy", "Vz"):
+            np.save(os.path.join(d, "Gathers", f"modData{k}.{comp}.npy"), getattr(self.modGather, comp))
+            np.save(os.path.join(d, "Gathers", f"resData{k}.{comp}.npy"), getattr(self.resGather, comp))
 
     # ---------------------------------------------------------------- Vp/Vs/Rho FWI
     def _all_shots_engine(self, listaTM):
@@ -677,6 +700,62 @@ class Elastic3D:
         np.save(os.path.join(d, "CostFunction", f"costFunction_{fq}Hz.npy"), self.costFunction)
         for name, g in (("gRho", gR), ("gMu", gM), ("gLambda", gL)):
             np.save(os.path.join(d, "Gradients", f"{name}_{fq}Hz.npy"), g.cpu().numpy())
+
+
+def observed_data(mTarget, geometry, wavelet, cpml, listTM):
+    """Observed gathers of every earthquake on the true model, one batched forward solve
+    (the reference's per-earthquake forwardFields('obs') loop, :3157-3185).  With
+    torch.distributed each rank models its shard and the list is gathered on every rank."""
+    e = Elastic3D(mTarget, geometry, wavelet, cpml, mode=1)
+    e.setModel(mTarget)
+    eng = e._all_shots_engine(listTM)
+    lo, hi = e._shard
+    out = [None] * geometry.getLenSismos()
+    if len(eng):
+        buf = eng.forward()
+        for i in range(hi - lo):
+            g = eng.gather_view(buf, i).cpu().numpy()
+            G = Gather(g.shape[1], g.shape[2])
+            G.Vx, G.Vy, G.Vz = g[0].copy(), g[1].copy(), g[2].copy()
+            out[lo + i] = G
+    eng.close()
+    rank, ws = _dist.world()
+    if ws > 1:
+        import torch.distributed as dist
+        parts = [None] * ws
+        dist.all_gather_object(parts, out[lo:hi])
+        for r, part in enumerate(parts):
+            a, _ = _dist.shard(len(out), r, ws)
+            out[a:a + len(part)] = part
+    return out
+
+
+def multifrequency_fwi(mTarget, cn, geometry, multFq, tprop, lenPML, listTM, nIteFWI, dt=None,
+                       results_dir=None, **fwi_kwargs):
+    """The reference's frequency continuation (mode 1 of the main program, :3134-3213): for
+    each frequency of ``multFq`` in order, a new Ricker wavelet and CPML, observed data on the
+    true model, then ``fwi_Vp_Vs_Rho`` continuing from the model the previous frequency
+    reached.  Returns {fq: cost history}; ``cn`` holds the final model."""
+    history = {}
+    for fq in multFq:
+        cn.MaxMinVp()
+        wavelet = Wavelet(fq, tprop, mTarget, dt=dt)
+        wavelet.ricker()
+        cpml = CPML(lenPML, wavelet, mTarget)
+        obs = observed_data(mTarget, geometry, wavelet, cpml, listTM)
+        if results_dir and _dist.world()[0] == 0:
+            os.makedirs(os.path.join(results_dir, "Gathers"), exist_ok=True)
+            np.save(os.path.join(results_dir, "Gathers", f"obsData_{fq}Hz.npy"),
+                    np.array([[g.Vx, g.Vy, g.Vz] for g in obs]))
+        e = Elastic3D(cn, geometry, wavelet, cpml, mode=1, results_dir=results_dir)
+        e.setModel(cn)
+        history[fq] = list(e.fwi_Vp_Vs_Rho(obs, listTM, nIteFWI, **fwi_kwargs))
+        cn.Rho = e.mk.Rho.copy()
+        cn.Lambda = e.mk.Lambda.copy()
+        cn.Mu = e.mk.Mu.copy()
+        cn.compute_Vp_Vs()
+        cn.hostToDevice()
+    return history
 
 
 def _sumsq(t):

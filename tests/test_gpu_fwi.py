@@ -71,3 +71,49 @@ def test_fwi_Vp_Vs_Rho_matches_reference(golden_refscale, cuda):
     assert rel_err(gL, d["fwi_glambda"]) < 5e-4
     assert rel_err(gM, d["fwi_gmu"]) < 5e-4
     assert rel_err(gR, d["fwi_grho"]) < 5e-4
+
+
+def test_observed_data_multifrequency_and_result_files(golden_refscale, cuda, tmp_path):
+    """Batched observed data equal the reference's gathers; the frequency-continuation
+    driver runs two frequencies and writes the reference's result files."""
+    from elastic_fm_vp_vs_rho_b200 import StressTensor, multifrequency_fwi, observed_data
+    d = golden_refscale
+    mt, m0, w, cp, geo = _setup(d)
+    tm = [StressTensor(*d["mt_obs"])] * len(d["src"])
+    obs = observed_data(mt, geo, w, cp, tm)
+    for k in range(len(d["src"])):
+        assert rel_err(np.stack([obs[k].Vx, obs[k].Vy, obs[k].Vz]), d[f"obs{k}"]) < 2e-5
+    fqs = [float(d["fq"]), 1.5 * float(d["fq"])]
+    hist = multifrequency_fwi(mt, m0, geo, fqs, 14.0, int(d["lenpml"]), tm, 1,
+                              results_dir=str(tmp_path), lbfgsLayers=4, ite_cte=2)
+    assert list(hist) == fqs and all(np.all(np.isfinite(h)) for h in hist.values())
+    for fq in fqs:
+        for f in (f"Gathers/obsData_{fq}Hz.npy", f"Models/Vp_{fq}Hz.npy", f"Models/Mu_{fq}Hz.npy",
+                  f"CostFunction/costFunction_{fq}Hz.npy", f"Gradients/gLambda_{fq}Hz.npy"):
+            assert (tmp_path / f).exists(), f
+    assert np.load(tmp_path / f"Gathers/obsData_{fqs[0]}Hz.npy").shape[:2] == (len(d["src"]), 3)
+    assert not np.array_equal(m0.Lambda, d["lam0"])  # the model moved
+
+
+def test_cross_correlation_through_elastic3d(golden_refscale, cuda, tmp_path):
+    import efm_oracle as O
+    from elastic_fm_vp_vs_rho_b200 import Elastic3D, StressTensor
+    d = golden_refscale
+    mt, m0, w, cp, geo = _setup(d)
+    e = Elastic3D(m0, geo, w, cp, mode=0, results_dir=str(tmp_path))
+    e.setModel(m0)
+    e.setStressTensor(StressTensor(*d["mt_mod"]))
+    e.setIdxEarthquake(0)
+    e.obsGather.Vx, e.obsGather.Vy, e.obsGather.Vz = d["obs0"]
+    e.forwardFields("mod")
+    e.computeResidualCrossCorrelation()
+    e.computeCostFunctionCrossCorrelation(0)
+    res, cost = O.xcorr_misfit(e.modGather.stack(), d["obs0"])
+    assert rel_err(e.resGather.stack(), res) < 2e-5
+    assert abs(e.costFunction[-1] - cost) <= 1e-6 * max(1.0, abs(cost))
+    e.costFunction = []
+    e.fwi_Mij(1)
+    for comp in ("Vx", "Vy", "Vz"):
+        assert (tmp_path / f"Gathers/modData0.{comp}.npy").exists()
+        assert (tmp_path / f"Gathers/resData0.{comp}.npy").exists()
+    assert (tmp_path / "TM/Mmodxx0.npy").exists() and (tmp_path / "CostFunction/costFunction0.npy").exists()

@@ -106,6 +106,7 @@ SIGNATURES = {
     "efm_conv3d_backward_weights": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _P, _P,
                                          ctypes.c_size_t, _P]),
     "efm_conv3d_status": (_I, [_P]),
+    "efm_conv3d_set_grouped_loads": (None, [_I]),
 }
 
 _lock = threading.Lock()

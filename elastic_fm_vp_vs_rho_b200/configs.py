@@ -261,3 +261,56 @@ def reference_default():
     shot = Shot(50, 52, 2, (1.0, 0.0, 1.0, 0.0, 0.0, 0.0), rx, ry, rz, nt)
     return Workload("reference_default_100x100x100", n, n, n, 1e3, 20, 0.1, dt, nt, vp, vs, rho,
                     [shot])
+
+
+@dataclasses.dataclass
+class Instance:
+    """One self-contained modelling instance of a heterogeneous batch."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    lenpml: int
+    fq: float
+    dt: float
+    nt: int
+    vp: np.ndarray
+    vs: np.ndarray
+    rho: np.ndarray
+    src: np.ndarray        # (nsrc, 3) cells
+    mt: np.ndarray         # (nsrc, 6)
+    rec: np.ndarray        # (nrec, 3) cells
+
+    @property
+    def ncells(self):
+        return self.nx * self.ny * self.nz
+
+
+def uneven_instances(seed=4, n=48, size_lo=(64, 64, 64), size_hi=(160, 160, 96), nt_per_s=None):
+    """Heterogeneous batch: n instances with seeded grid sizes between size_lo and size_hi
+    (x, y multiples of 8), dx 10-20 m, 1-4 MT sources at 200-800 m depth, 7-15 Hz Ricker,
+    64-256 surface receivers; record length 1.2 s of propagation at each instance's dt."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx = int(rng.integers(size_lo[0] // 8, size_hi[0] // 8 + 1)) * 8
+        ny = int(rng.integers(size_lo[1] // 8, size_hi[1] // 8 + 1)) * 8
+        nz = int(rng.integers(size_lo[2], size_hi[2] + 1))
+        dx = float(rng.uniform(10.0, 20.0))
+        W = 10
+        vp, vs, rho = layered_anomaly_model(ny, nz, nx, dx, seed * 1000 + k, n_layers=4,
+                                            n_anomalies=2, sigma_m=4 * dx, vpvs=1.75)
+        dt = cfl_dt(dx, float(vp.max()))
+        fq = float(rng.uniform(7.0, 15.0))
+        nt = int(round((1.2 if nt_per_s is None else nt_per_s) / dt))
+        nsrc = int(rng.integers(1, 5))
+        zmax = min(nz - W - 3, int(800.0 / dx))
+        zmin = min(zmax, max(3, int(200.0 / dx)))
+        src = np.stack([rng.integers(W + 3, nx - W - 3, nsrc), rng.integers(W + 3, ny - W - 3, nsrc),
+                        rng.integers(zmin, zmax + 1, nsrc)], axis=1).astype(np.int32)
+        mt = np.stack([random_moment_tensor(rng) for _ in range(nsrc)])
+        side = int(rng.integers(8, 17))
+        rx, ry, rz = surface_receivers(nx, ny, W, side, side)
+        out.append(Instance(nx, ny, nz, dx, W, fq, dt, nt, vp, vs, rho, src, mt,
+                            np.stack([rx, ry, rz], axis=1)))
+    return out

@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(CV_THREADS, 1)
 efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_w,
                     int nx, int ny, int nz, const float *__restrict__ bias, int relu,
                     const __nv_bfloat16 *__restrict__ mask, __nv_bfloat16 *__restrict__ y_bf16,
-                    float *__restrict__ y_f32) {
+                    float *__restrict__ y_f32, int grouped) {
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 64 && CIN <= 64, "channels");
     constexpr int NG = CIN / 8;                       // 8-channel groups (K core matrices)
     constexpr int WBYTES = 27 * CIN * COUT * 2;
@@ -195,9 +195,12 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
                 if (!cv_wait(&S.empty[st], ph ^ 1u, abort)) { ok = false; break; }
                 efm_mbar_expect_tx(&S.full[st], ASTAGE);
                 unsigned char *dst = asm_ + st * ASTAGE;
-                for (int g = 0; g < NG; ++g)
-                    efm_tma_load_4d(dst + g * CV_ASLAB, &tm_x, &S.full[st], 8 * g, x0 - 4,
-                                    z0 + zi - 1, y + kd - 1);
+                if (grouped)  // every 8-channel slab in one box (5-D map, group = dim 4)
+                    efm_tma_load_5d(dst, &tm_x, &S.full[st], 0, x0 - 4, z0 + zi - 1, y + kd - 1, 0);
+                else
+                    for (int g = 0; g < NG; ++g)
+                        efm_tma_load_4d(dst + g * CV_ASLAB, &tm_x, &S.full[st], 8 * g, x0 - 4,
+                                        z0 + zi - 1, y + kd - 1);
                 issued[st] = true;
                 issued_parity[st] = ph;
                 if (++st == NST) { st = 0; ph ^= 1u; }
@@ -311,7 +314,7 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(CV_THREADS, 1)
 efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_dy,
-                      int nx, int ny, int nz, float *__restrict__ partial) {
+                      int nx, int ny, int nz, float *__restrict__ partial, int grouped) {
     constexpr int NPAIR = 128 / CIN;               // (kd, kh) pairs per M tile
     constexpr int NGI = CIN / 8, NGO = COUT / 8;
     constexpr int ASTAGE = NPAIR * NGI * WG_ASLAB;  // 16 slabs
@@ -347,12 +350,18 @@ efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_con
                 const int pi = q * NPAIR + lp;  // (kd, kh) = (pi / 3, pi % 3); pi > 8: zero rows
                 const int zz = pi < 9 ? z + pi % 3 - 1 : -64;
                 const int yy = pi < 9 ? y + pi / 3 - 1 : -64;
-                for (int g = 0; g < NGI; ++g)
-                    efm_tma_load_4d(dst + (lp * NGI + g) * WG_ASLAB, &tm_x, &S.full[st], 8 * g,
-                                    x0 - 4, zz, yy);
+                if (grouped)
+                    efm_tma_load_5d(dst + lp * NGI * WG_ASLAB, &tm_x, &S.full[st], 0, x0 - 4, zz, yy, 0);
+                else
+                    for (int g = 0; g < NGI; ++g)
+                        efm_tma_load_4d(dst + (lp * NGI + g) * WG_ASLAB, &tm_x, &S.full[st], 8 * g,
+                                        x0 - 4, zz, yy);
             }
-            for (int g = 0; g < NGO; ++g)
-                efm_tma_load_4d(dst + ASTAGE + g * WG_BSLAB, &tm_dy, &S.full[st], 8 * g, x0, z, y);
+            if (grouped)
+                efm_tma_load_5d(dst + ASTAGE, &tm_dy, &S.full[st], 0, x0, z, y, 0);
+            else
+                for (int g = 0; g < NGO; ++g)
+                    efm_tma_load_4d(dst + ASTAGE + g * WG_BSLAB, &tm_dy, &S.full[st], 8 * g, x0, z, y);
             issued[st] = true;
             issued_parity[st] = ph;
             if (++st == CV_STAGES) { st = 0; ph ^= 1u; }
@@ -486,6 +495,22 @@ PFN_cuTensorMapEncodeTiled_v12000 conv_encoder() {
     return fn;
 }
 
+// channels-last BF16 volume (ny, nz, nx, c) seen as 5-D (8 channels, x, z, y, c / 8 groups)
+// with a box holding every group: one TMA copy per slab set.  false when the driver
+// rejects the layout (the group stride, 16 bytes, is smaller than the others).
+bool map_volume_grouped(CUtensorMap *m, const void *base, const efm_conv_desc *d, int c, int rows) {
+    auto enc = conv_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[5] = {8, (cuuint64_t)d->nx, (cuuint64_t)d->nz, (cuuint64_t)d->ny, (cuuint64_t)c / 8};
+    cuuint64_t strides[4] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * d->nx,
+                             (cuuint64_t)c * 2 * d->nx * d->nz, 16};
+    cuuint32_t box[5] = {8, (cuuint32_t)rows, 1, 1, (cuuint32_t)c / 8};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box,
+               es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // channels-last BF16 volume (ny, nz, nx, c); box (8 channels, rows along x, 1, 1)
 int map_volume(CUtensorMap *m, const void *base, const efm_conv_desc *d, int c, int rows) {
     auto enc = conv_encoder();
@@ -519,6 +544,9 @@ int map_weights(CUtensorMap *m, const void *base, int cin, int cout) {
     return EFM_OK;
 }
 
+// 1: one 5-D TMA copy per slab set when the driver accepts the map; 0: per-group copies
+int g_grouped_ok = 1;
+
 bool chan_ok(int c) { return c == 16 || c == 32 || c == 64; }
 
 int check_desc(const efm_conv_desc *d) {
@@ -541,7 +569,7 @@ int num_sms() {
 
 template <int CIN, int COUT, int MODE>
 int launch_fwd(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tw, const float *bias,
-               int relu, const void *mask, void *yb, float *yf, cudaStream_t s) {
+               int relu, const void *mask, void *yb, float *yf, int grouped, cudaStream_t s) {
     const int smem_need = 27 * CIN * COUT * 2 +
                           cv_fwd_stages(27 * CIN * COUT * 2, (CIN / 8) * CV_ASLAB) * (CIN / 8) * CV_ASLAB;
     const int smem = smem_need > CV_MIN_SMEM ? smem_need : CV_MIN_SMEM;
@@ -552,17 +580,18 @@ int launch_fwd(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap 
     const int grid = (int)(tiles < num_sms() ? tiles : num_sms());
     k<<<grid, CV_THREADS, smem, s>>>(tx, tw, d->nx, d->ny, d->nz, bias, relu,
                                       static_cast<const __nv_bfloat16 *>(mask),
-                                      static_cast<__nv_bfloat16 *>(yb), yf);
+                                      static_cast<__nv_bfloat16 *>(yb), yf, grouped);
     e = cudaGetLastError();
     return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
 }
 
 template <int MODE>
 int dispatch_fwd(int cin, int cout, const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tw,
-                 const float *bias, int relu, const void *mask, void *yb, float *yf, cudaStream_t s) {
+                 const float *bias, int relu, const void *mask, void *yb, float *yf, int grouped,
+                 cudaStream_t s) {
 #define EFM_CONV_CASE(A, B)                                                           \
     if (cin == A && cout == B)                                                        \
-        return launch_fwd<A, B, MODE>(d, tx, tw, bias, relu, mask, yb, yf, s);
+        return launch_fwd<A, B, MODE>(d, tx, tw, bias, relu, mask, yb, yf, grouped, s);
     EFM_CONV_CASE(16, 16) EFM_CONV_CASE(16, 32) EFM_CONV_CASE(16, 64)
     EFM_CONV_CASE(32, 16) EFM_CONV_CASE(32, 32) EFM_CONV_CASE(32, 64)
     EFM_CONV_CASE(64, 16) EFM_CONV_CASE(64, 32)
@@ -581,7 +610,7 @@ int wgrad_nq(int cin) { return (9 + 128 / cin - 1) / (128 / cin); }
 
 template <int CIN, int COUT>
 int launch_wgrad(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tdy, float *part,
-                 int nsplit, cudaStream_t s) {
+                 int nsplit, int grouped, cudaStream_t s) {
     constexpr int stage = (128 / CIN) * (CIN / 8) * WG_ASLAB + (COUT / 8) * WG_BSLAB;
     const int smem_need = CV_STAGES * stage;
     const int smem = smem_need > CV_MIN_SMEM ? smem_need : CV_MIN_SMEM;
@@ -589,7 +618,7 @@ int launch_wgrad(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMa
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
     dim3 grid(nsplit, wgrad_nq(CIN));
-    k<<<grid, CV_THREADS, smem, s>>>(tx, tdy, d->nx, d->ny, d->nz, part);
+    k<<<grid, CV_THREADS, smem, s>>>(tx, tdy, d->nx, d->ny, d->nz, part, grouped);
     e = cudaGetLastError();
     return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
 }
@@ -621,9 +650,10 @@ int efm_conv3d_forward(const efm_conv_desc *d, const void *x, const void *w_bf16
     if (!al16(x) || !al16(w_bf16) || !al16(y_bf16) || !al16(y_f32))
         return efm_internal_fail(EFM_ERR_ARG, "buffers must be 16-byte aligned");
     CUtensorMap tx, tw;
-    if ((rc = map_volume(&tx, x, d, d->cin, CV_AROWS))) return rc;
+    const int grouped = g_grouped_ok && map_volume_grouped(&tx, x, d, d->cin, CV_AROWS);
+    if (!grouped && (rc = map_volume(&tx, x, d, d->cin, CV_AROWS))) return rc;
     if ((rc = map_weights(&tw, w_bf16, d->cin, d->cout))) return rc;
-    return dispatch_fwd<0>(d->cin, d->cout, d, tx, tw, bias, relu, nullptr, y_bf16, y_f32,
+    return dispatch_fwd<0>(d->cin, d->cout, d, tx, tw, bias, relu, nullptr, y_bf16, y_f32, grouped,
                            (cudaStream_t)stream);
 }
 
@@ -638,9 +668,10 @@ int efm_conv3d_backward_data(const efm_conv_desc *d, const void *dy, const void 
     t.cin = d->cout;
     t.cout = d->cin;
     CUtensorMap tx, tw;
-    if ((rc = map_volume(&tx, dy, &t, t.cin, CV_AROWS))) return rc;
+    const int grouped = g_grouped_ok && map_volume_grouped(&tx, dy, &t, t.cin, CV_AROWS);
+    if (!grouped && (rc = map_volume(&tx, dy, &t, t.cin, CV_AROWS))) return rc;
     if ((rc = map_weights(&tw, wt_bf16, t.cin, t.cout))) return rc;
-    return dispatch_fwd<1>(t.cin, t.cout, &t, tx, tw, nullptr, 0, relu_mask, dx, nullptr,
+    return dispatch_fwd<1>(t.cin, t.cout, &t, tx, tw, nullptr, 0, relu_mask, dx, nullptr, grouped,
                            (cudaStream_t)stream);
 }
 
@@ -661,13 +692,15 @@ int efm_conv3d_backward_weights(const efm_conv_desc *d, const void *x, const voi
         return efm_internal_fail(EFM_ERR_ARG, "buffers must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
     CUtensorMap tx, tdy;
-    if ((rc = map_volume(&tx, x, d, d->cin, WG_AROWS))) return rc;
-    if ((rc = map_volume(&tdy, dy, d, d->cout, WG_K))) return rc;
+    const int grouped = g_grouped_ok && map_volume_grouped(&tx, x, d, d->cin, WG_AROWS) &&
+                        map_volume_grouped(&tdy, dy, d, d->cout, WG_K);
+    if (!grouped && (rc = map_volume(&tx, x, d, d->cin, WG_AROWS))) return rc;
+    if (!grouped && (rc = map_volume(&tdy, dy, d, d->cout, WG_K))) return rc;
     const int nq = wgrad_nq(d->cin), nsplit = wgrad_splits(d, nq);
     float *part = static_cast<float *>(workspace);
     rc = EFM_ERR_ARG;
 #define EFM_WG_CASE(A, B) \
-    if (d->cin == A && d->cout == B) rc = launch_wgrad<A, B>(d, tx, tdy, part, nsplit, s);
+    if (d->cin == A && d->cout == B) rc = launch_wgrad<A, B>(d, tx, tdy, part, nsplit, grouped, s);
     EFM_WG_CASE(16, 16) EFM_WG_CASE(16, 32) EFM_WG_CASE(16, 64)
     EFM_WG_CASE(32, 16) EFM_WG_CASE(32, 32) EFM_WG_CASE(32, 64)
     EFM_WG_CASE(64, 16) EFM_WG_CASE(64, 32)
@@ -684,6 +717,8 @@ int efm_conv3d_backward_weights(const efm_conv_desc *d, const void *x, const voi
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
 }
+
+void efm_conv3d_set_grouped_loads(int enable) { g_grouped_ok = enable != 0; }
 
 int efm_conv3d_status(void *stream) {
     cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);

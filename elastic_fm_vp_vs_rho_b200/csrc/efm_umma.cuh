@@ -108,3 +108,13 @@ __device__ __forceinline__ void efm_tma_load_4d(void *dst, const CUtensorMap *m,
         "l"(m), "r"(efm_smem_addr(bar)), "r"(c), "r"(x), "r"(z), "r"(y)
         : "memory");
 }
+
+// 5-D tile load (c, x, z, y, channel group), c innermost, completing on bar.
+__device__ __forceinline__ void efm_tma_load_5d(void *dst, const CUtensorMap *m, uint64_t *bar,
+                                                int c, int x, int z, int y, int g) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(efm_smem_addr(dst)),
+        "l"(m), "r"(efm_smem_addr(bar)), "r"(c), "r"(x), "r"(z), "r"(y), "r"(g)
+        : "memory");
+}

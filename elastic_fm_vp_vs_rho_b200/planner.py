@@ -1,0 +1,88 @@
+"""Memory planner: split a set of instances into sub-batches that fit a device budget.
+
+A batch keeps, per instance, the wavefields and their adjoints in HBM plus whatever the
+gradient needs from the forward run: the boundary strips of the reverse-time rebuild
+(nt x 3 x S floats, S = 4 (by bz + bz bx + by bx) over the non-CPML box) for the
+reference's imaging gradient, or full-state checkpoints every K steps plus one segment of
+K + 1 stored steps for the exact gradient.  :func:`instance_bytes` restates those
+allocations (efm_capi.cu: ensure_workspace, ensure_exact) plus the caller's buffers
+(gathers, residual, gradient); :func:`plan` packs instances into sub-batches (first fit,
+largest first) under ``budget`` bytes; :func:`choose_checkpoint_interval` picks the
+smallest checkpoint interval K whose exact-gradient workspace fits.
+"""
+from __future__ import annotations
+
+import math
+
+
+def _geometry(nx, ny, nz, lenpml):
+    W = lenpml
+    ncell = nx * ny * nz
+    psi = 6 * (ny * nz * 2 * W + 2 * W * nz * nx + ny * W * nx)
+    bx, by, bz = nx - 2 * W, ny - 2 * W, nz - W - 2
+    strip = 4 * by * bz + 4 * bz * bx + 4 * by * bx
+    return ncell, psi, strip
+
+
+def instance_bytes(nx, ny, nz, lenpml, nt, nrec=0, gradient="imaging", ck_every=50):
+    """Device bytes one instance needs for forward + gradient.
+
+    gradient: "none" (forward only), "imaging" (reference-mode gradient from strips) or
+    "exact" (checkpointed exact adjoint with interval ck_every)."""
+    ncell, psi, strip = _geometry(nx, ny, nz, lenpml)
+    b = 2 * ncell * 4                       # 1/mu, 1/rho
+    b += psi * 4
+    gathers = 3 * nt * nrec * 4
+    if gradient == "none":
+        return b + 9 * ncell * 4 + gathers
+    b += 21 * ncell * 4                     # forward, rebuild ping-pong and adjoint fields
+    b += 3 * ncell * 4 + 2 * gathers        # gradient output, gathers + residual
+    if gradient == "imaging":
+        b += nt * 3 * strip * 4
+    elif gradient == "exact":
+        K = max(1, min(ck_every, nt))
+        nck = (nt + K - 1) // K
+        b += nck * (9 * ncell + psi) * 4 + (K + 1) * 9 * ncell * 4 + 2 * psi * 4
+    else:
+        raise ValueError(f"unknown gradient kind {gradient!r}")
+    return b
+
+
+def choose_checkpoint_interval(nx, ny, nz, lenpml, nt, budget, nrec=0):
+    """Smallest-memory interval is ~sqrt(nt); returns the K minimising the exact-gradient
+    workspace if it fits ``budget``, else None."""
+    best, best_b = None, None
+    for K in range(1, nt + 1):
+        bb = instance_bytes(nx, ny, nz, lenpml, nt, nrec, "exact", K)
+        if best_b is None or bb < best_b:
+            best, best_b = K, bb
+        if K > 4 * math.isqrt(nt) + 4 and best_b is not None:
+            break
+    return best if best_b is not None and best_b <= budget else None
+
+
+def plan(sizes, budget):
+    """sizes: bytes per instance.  Returns sub-batches (lists of indices, each sub-batch in
+    ascending index order) whose totals are <= budget; raises if one instance alone does
+    not fit."""
+    order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
+    bins, loads = [], []
+    for i in order:
+        if sizes[i] > budget:
+            raise MemoryError(f"instance {i} needs {sizes[i]} bytes, budget is {budget}")
+        for b in range(len(bins)):
+            if loads[b] + sizes[i] <= budget:
+                bins[b].append(i)
+                loads[b] += sizes[i]
+                break
+        else:
+            bins.append([i])
+            loads.append(sizes[i])
+    return [sorted(b) for b in bins]
+
+
+def device_budget(fraction=0.85, reserve=2 << 30):
+    """Bytes of free device memory the planner may use."""
+    import torch
+    free, _ = torch.cuda.mem_get_info()
+    return max(0, int(free * fraction) - reserve)

@@ -318,6 +318,9 @@ EFM_API int efm_conv3d_backward_weights(const efm_conv_desc *d, const void *x_de
                                         void *workspace_dev, size_t workspace_bytes, void *stream);
 /* Synchronizes `stream`; EFM_ERR_TIMEOUT if a convolution kernel gave up a wait (cleared). */
 EFM_API int efm_conv3d_status(void *stream);
+/* 1 (default): stage all 8-channel slabs of an input row with one TMA copy (a 5-D tensor
+ * map) when the driver accepts that map; 0: one copy per slab.  Results are identical. */
+EFM_API void efm_conv3d_set_grouped_loads(int enable);
 
 #ifdef __cplusplus
 }

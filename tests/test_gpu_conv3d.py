@@ -116,3 +116,29 @@ def test_weight_layout_roundtrip_and_unsupported_pairs():
     rc = L.efm_conv3d_forward(ctypes.byref(d), None, None, None, 0, None, None, None)
     assert rc == _lib.EFM_ERR_ARG
     assert L.efm_conv3d_wgrad_workspace(ctypes.byref(d)) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cin,cout", [(32, 64), (64, 16)])
+def test_grouped_and_per_slab_loads_agree(cuda, cin, cout):
+    """One 5-D TMA copy per input row or one copy per 8-channel slab: identical results."""
+    import torch
+    from elastic_fm_vp_vs_rho_b200 import _lib, conv3d
+    x, w, b = _data((3, 6, 40), cin, cout, 11)
+    g = torch.Generator().manual_seed(12)
+    dy = torch.randn((3, 6, 40, cout), generator=g).to(torch.bfloat16).cuda()
+    wb, wt = conv3d.prep_weights(w.cuda())
+    L = _lib.load()
+    outs = []
+    for grouped in (1, 0):
+        L.efm_conv3d_set_grouped_loads(grouped)
+        try:
+            _, yf = conv3d.forward(x.cuda(), wb, b.cuda(), relu=True, out_bf16=False, out_f32=True)
+            dx = conv3d.backward_data(dy, wt, cin, relu_mask=x.cuda())
+            dw, db = conv3d.backward_weights(x.cuda(), dy)
+            conv3d.status()
+        finally:
+            L.efm_conv3d_set_grouped_loads(1)
+        outs.append((yf.cpu(), dx.cpu(), dw.cpu(), db.cpu()))
+    for a, c in zip(*outs):
+        assert torch.equal(a, c)

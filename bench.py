@@ -401,7 +401,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded layered + anomaly model, MT source)",
                 "config": dict(config_dict(w, args, world), launch_shape=tuned and {
-                    "tile_rows": tuned["rows"], "ychunk": tuned["ychunk"],
+                    "tile_rows": tuned["rows"], "ring": tuned.get("ring", 4), "ychunk": tuned["ychunk"],
                     "source": "autotuned (probe of %d steps)" % tuned["nt_probe"]}),
                 "gpu_launches": gpu_launches,
                 "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}

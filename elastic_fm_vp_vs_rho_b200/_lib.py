@@ -29,6 +29,7 @@ EFM_SAVE_STRIPS = 1
 EFM_SAVE_CHECKPOINTS = 2
 EFM_OPT_CHECKPOINT_EVERY = 3
 EFM_OPT_TILE_ROWS = 4
+EFM_OPT_RING_DEPTH = 5
 EFM_NKERN = 9
 KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity",
                 "rev_stress", "residual_misfit", "model_reciprocals", "imaging")

@@ -1,9 +1,11 @@
 """Autotuner for the plane-streaming kernels' launch shape, with a JSON cache.
 
-Two knobs decide how the stress/velocity kernels map a batch onto the 148 SMs: the tile
+Three knobs decide how the stress/velocity kernels map a batch onto the 148 SMs: the tile
 height (``EFM_OPT_TILE_ROWS``: 64 x 8 tiles with two cells per thread and two blocks per SM,
-or 64 x 4 tiles with one cell per thread and three blocks per SM) and the planes each block
-marches along y (``EFM_OPT_YCHUNK``; 0 = the wave-filling heuristic).  :func:`tune` times a
+or 64 x 4 tiles with one cell per thread), the shared-memory ring depth
+(``EFM_OPT_RING_DEPTH``: 4, or 6 with one-row tiles -- more planes in flight, fewer blocks)
+and the planes each block marches along y (``EFM_OPT_YCHUNK``; 0 = the wave-filling
+heuristic).  :func:`tune` times a
 short probe of the batch -- the same grids, sources and receivers, ``nt_probe`` steps of
 forward (with strips) + misfit + model/MT gradient -- for every candidate, applies the
 fastest to the batch and caches it under a key made of the device name and the instance
@@ -20,7 +22,9 @@ import numpy as np
 
 from . import _lib
 
-DEFAULT_CANDIDATES = tuple((rows, yc) for rows in (2, 1) for yc in (0, 8, 16, 32))
+# (tile rows, ring depth, y-chunk)
+DEFAULT_CANDIDATES = tuple((rows, ring, yc) for rows, ring in ((2, 4), (1, 4), (1, 6))
+                           for yc in (0, 8, 16, 32))
 
 
 def cache_path() -> str:
@@ -58,6 +62,7 @@ def save_cache(cache: dict, path=None):
 
 def apply(batch, choice: dict):
     batch.set_option(_lib.EFM_OPT_TILE_ROWS, int(choice["rows"]))
+    batch.set_option(_lib.EFM_OPT_RING_DEPTH, int(choice.get("ring", 4)))
     batch.set_option(_lib.EFM_OPT_YCHUNK, int(choice["ychunk"]))
 
 
@@ -108,11 +113,12 @@ def tune(batch, nt_probe=48, candidates=DEFAULT_CANDIDATES, use_cache=True, path
     obs = torch.zeros(probe.gather_size, device="cuda")
     best = None
     times = {}
-    for rows, yc in candidates:
-        ms = time_choice(probe, {"rows": rows, "ychunk": yc}, obs, repeats)
-        times[f"{rows}x{yc}"] = ms
+    for cand in candidates:
+        rows, ring, yc = cand if len(cand) == 3 else (cand[0], 4, cand[1])
+        ms = time_choice(probe, {"rows": rows, "ring": ring, "ychunk": yc}, obs, repeats)
+        times[f"rows{rows}_ring{ring}_y{yc}"] = ms
         if best is None or ms < best["ms"]:
-            best = {"rows": rows, "ychunk": yc, "ms": ms}
+            best = {"rows": rows, "ring": ring, "ychunk": yc, "ms": ms}
     probe.close()
     best["nt_probe"] = int(min(nt_probe, max(s["nt"] for s in batch.specs)))
     best["candidates_ms"] = {k: float(np.round(v, 4)) for k, v in times.items()}

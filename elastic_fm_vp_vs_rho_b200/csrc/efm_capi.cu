@@ -22,8 +22,9 @@ extern "C" cudaError_t efm_launch_stress(int pass, const EfmInst *insts, int nin
                                          int it, cudaStream_t s);
 extern "C" cudaError_t efm_launch_velocity(int pass, const EfmInst *insts, int ninst, int tiles,
                                            int it, cudaStream_t s);
-extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, const EfmInst *insts,
-                                         int ninst, int tiles, int it, cudaStream_t s);
+extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, int ring,
+                                         const EfmInst *insts, int ninst, int tiles, int it,
+                                         cudaStream_t s);
 extern "C" cudaError_t efm_stream_init_attributes();
 extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int tiles, int it,
                                         cudaStream_t s);
@@ -143,7 +144,9 @@ struct efm_ctx {
     int opt_stream = 1;
     int opt_ychunk = 0;
     int opt_rows = 0;
+    int opt_ring = 0;
     int rows = 2;  // cells per thread of the tables last built for the streaming kernels
+    int ring = 4;  // ring depth of those tables' kernels
     int opt_ck_every = 50;
     EfmExact *d_ex = nullptr;  // exact-adjoint tables, two (memory-variable parities) per instance
     int ex_cap = 0;
@@ -503,8 +506,9 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
     const bool st = stream_ok(ctx);
     if (st && (rc = get_encoder())) return rc;
     const int rows = ctx->rows = ctx->opt_rows == 1 ? 1 : 2;
+    const int ring = ctx->ring = (rows == 1 && ctx->opt_ring == 6) ? 6 : 4;
     const int tz = efm_st_tz(rows), hz = efm_st_hz(rows);
-    const int yc = st ? choose_ychunk(ctx, tz, rows == 1 ? 3 : 2) : 0;
+    const int yc = st ? choose_ychunk(ctx, tz, efm_stream_blocks(rows, ring)) : 0;
     std::vector<EfmInst> tab(2 * (size_t)n);
     std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
     for (int i = 0; i < n; ++i) {
@@ -566,12 +570,12 @@ int forward_step(efm_ctx *ctx, bool st, int it, cudaStream_t s) {
     const EfmInst *ts = ctx->d_tab, *tv = ctx->d_tab + n;
     int rc;
     if ((rc = timed_launch(ctx, EFM_K_FWD_STRESS, s, [&] {
-             return st ? efm_launch_stream(EFM_FWD, 0, ctx->rows, ts, n, ctx->tiles[T_FWD_S], it, s)
+             return st ? efm_launch_stream(EFM_FWD, 0, ctx->rows, ctx->ring, ts, n, ctx->tiles[T_FWD_S], it, s)
                        : efm_launch_stress(EFM_FWD, ts, n, ctx->tiles[T_FWD_S], it, s);
          })))
         return rc;
     return timed_launch(ctx, EFM_K_FWD_VELOCITY, s, [&] {
-        return st ? efm_launch_stream(EFM_FWD, 1, ctx->rows, tv, n, ctx->tiles[T_FWD_V], it, s)
+        return st ? efm_launch_stream(EFM_FWD, 1, ctx->rows, ctx->ring, tv, n, ctx->tiles[T_FWD_V], it, s)
                   : efm_launch_velocity(EFM_FWD, tv, n, ctx->tiles[T_FWD_V], it, s);
     });
 }
@@ -951,8 +955,9 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     const bool st = stream_ok(ctx);
     if (st && (rc = get_encoder())) return rc;
     const int rows = ctx->rows = ctx->opt_rows == 1 ? 1 : 2;
+    const int ring = ctx->ring = (rows == 1 && ctx->opt_ring == 6) ? 6 : 4;
     const int tz = efm_st_tz(rows), hz = efm_st_hz(rows);
-    const int yc = st ? choose_ychunk(ctx, tz, rows == 1 ? 3 : 2) : 0;
+    const int yc = st ? choose_ychunk(ctx, tz, efm_stream_blocks(rows, ring)) : 0;
     const int yci = st ? choose_ychunk(ctx, EFM_IMG_TZ, 3) : 0;
     std::vector<EfmInst> tab((size_t)T_NSLOT * n);
     std::vector<CUtensorMap> maps(st ? (size_t)n * EFM_MAPS_PER_INST : 0);
@@ -1083,12 +1088,12 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     auto dtab = [&](int k) { return (const EfmInst *)(ctx->d_tab + (size_t)k * n); };
     for (int it = 0; it < maxsteps; ++it) {
         if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
-                 return st ? efm_launch_stream(EFM_ADJ, 0, ctx->rows, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
+                 return st ? efm_launch_stream(EFM_ADJ, 0, ctx->rows, ctx->ring, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
                            : efm_launch_stress(EFM_ADJ, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s);
              })))
             return rc;
         if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
-                 return st ? efm_launch_stream(EFM_ADJ, 1, ctx->rows, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s)
+                 return st ? efm_launch_stream(EFM_ADJ, 1, ctx->rows, ctx->ring, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s)
                            : efm_launch_velocity(EFM_ADJ, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s);
              })))
             return rc;
@@ -1097,7 +1102,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
             const int ki = (it & 1) ? T_IMG1 : T_IMG0;
             // stream kernels: rebuild, then imaging; otherwise one fused rebuild + imaging kernel
             if ((rc = timed_launch(ctx, EFM_K_REV_VELOCITY, s, [&] {
-                     return st ? efm_launch_stream(EFM_REV, 1, ctx->rows, dtab(kv), n, ctx->tiles[kv], it, s)
+                     return st ? efm_launch_stream(EFM_REV, 1, ctx->rows, ctx->ring, dtab(kv), n, ctx->tiles[kv], it, s)
                                : efm_launch_velocity(EFM_REV, dtab(kv), n, ctx->tiles[kv], it, s);
                  })))
                 return rc;
@@ -1106,7 +1111,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                        })))
                 return rc;
             if ((rc = timed_launch(ctx, EFM_K_REV_STRESS, s, [&] {
-                     return st ? efm_launch_stream(EFM_REV, 0, ctx->rows, dtab(ks), n, ctx->tiles[ks], it, s)
+                     return st ? efm_launch_stream(EFM_REV, 0, ctx->rows, ctx->ring, dtab(ks), n, ctx->tiles[ks], it, s)
                                : efm_launch_stress(EFM_REV, dtab(ks), n, ctx->tiles[ks], it, s);
                  })))
                 return rc;
@@ -1133,6 +1138,10 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
         case EFM_OPT_TILE_ROWS:
             if (value < 0 || value > 2) return fail(EFM_ERR_ARG, "tile rows must be 0, 1 or 2");
             ctx->opt_rows = value;
+            break;
+        case EFM_OPT_RING_DEPTH:
+            if (value != 0 && value != 4 && value != 6) return fail(EFM_ERR_ARG, "ring depth must be 0, 4 or 6");
+            ctx->opt_ring = value;
             break;
         default: return fail(EFM_ERR_ARG, "unknown option");
     }

@@ -29,7 +29,7 @@ __device__ __forceinline__ float frcp(float a) {
     return r;
 }
 
-template <int ROWS>
+template <int ROWS, int SR>
 struct Ring {
     static constexpr int HB = efm_halo_bytes(ROWS), CB = efm_center_bytes(ROWS);
     unsigned char *base;
@@ -37,8 +37,8 @@ struct Ring {
     int stage_bytes;
     int nh;
     int p0;  // plane held by stage 0 at its first use
-    __device__ __forceinline__ int stage(int p) const { return (p - p0) & (EFM_SR - 1); }
-    __device__ __forceinline__ uint32_t parity(int p) const { return ((p - p0) / EFM_SR) & 1; }
+    __device__ __forceinline__ int stage(int p) const { return (p - p0) % SR; }
+    __device__ __forceinline__ uint32_t parity(int p) const { return ((p - p0) / SR) & 1; }
     __device__ __forceinline__ const float *halo(int s, int f) const {
         return reinterpret_cast<const float *>(base + s * stage_bytes + f * HB);
     }
@@ -47,8 +47,8 @@ struct Ring {
     }
 };
 
-template <int ROWS, int NH, int NC>
-__device__ __forceinline__ void issue_plane(const Ring<ROWS> &R, const CUtensorMap *tm, int x0,
+template <int ROWS, int SR, int NH, int NC>
+__device__ __forceinline__ void issue_plane(const Ring<ROWS, SR> &R, const CUtensorMap *tm, int x0,
                                             int z0, int p) {
     constexpr int HB = efm_halo_bytes(ROWS), CB = efm_center_bytes(ROWS);
     const int s = R.stage(p);
@@ -82,18 +82,18 @@ __device__ __forceinline__ Tile stream_tile(const EfmInst &I, int block) {
     return t;
 }
 
-template <int ROWS>
-__device__ void drain(const Ring<ROWS> &R, int first, int last) {
+template <int ROWS, int SR>
+__device__ void drain(const Ring<ROWS, SR> &R, int first, int last) {
     for (int p = first; p <= last; ++p) efm_mbar_wait(&R.bar[R.stage(p)], R.parity(p), nullptr);
 }
 
 // Block set-up shared by both kernels: barriers, prologue loads, source flag, receiver bits.
-template <int ROWS, int NH, int NC>
-__device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ring<ROWS> &R,
+template <int ROWS, int SR, int NH, int NC>
+__device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ring<ROWS, SR> &R,
                                              const CUtensorMap *tm, int *s_flags,
                                              unsigned long long *s_recbits) {
     if (threadIdx.x == 0) {
-        for (int s = 0; s < EFM_SR; ++s) efm_mbar_init(&R.bar[s], 1);
+        for (int s = 0; s < SR; ++s) efm_mbar_init(&R.bar[s], 1);
         efm_fence_barrier_init();
         int f = 0;
         for (int s = 0; s < I.nsrc; ++s)
@@ -122,16 +122,21 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int q = 0; q < NH + NC; ++q) efm_prefetch_tmap(tm + q);
-        for (int p = R.p0; p <= min(T.ye, R.p0 + EFM_SR - 1); ++p)
-            issue_plane<ROWS, NH, NC>(R, tm, T.x0, T.z0, p);
+        for (int p = R.p0; p <= min(T.ye, R.p0 + SR - 1); ++p)
+            issue_plane<ROWS, SR, NH, NC>(R, tm, T.x0, T.z0, p);
     }
 }
 
 // ------------------------------------------------------------------------------ stress
-template <int PASS, int ROWS>
-__device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS> &R, int sm, int s0,
+// CPML coefficients of one cell, loaded once per block (x, z) or per plane (y)
+struct Coef {
+    float ax, bx, ay, by, az, bz;
+};
+
+template <int PASS, int ROWS, int SR>
+__device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, SR> &R, int sm, int s0,
                                             int sp, int it, int x, int y, int z, int hidx,
-                                            int cidx, bool has_src, const float *pp) {
+                                            int cidx, bool has_src, const float *pp, const Coef &C) {
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
     const float *vx0 = R.halo(s0, 0), *vy0 = R.halo(s0, 1), *vz0 = R.halo(s0, 2);
     const float *rm0 = R.halo(s0, 3), *rm1 = R.halo(sp, 3);
@@ -153,7 +158,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS> &
             const int xs = x < W ? x : x - (nx - 2 * W);
             const int64_t st = (int64_t)ny * nz * 2 * W;
             float *p = I.psi_x + ((int64_t)y * nz + z) * (2 * W) + xs;
-            const float a = I.cpml[x], b = I.cpml[nx + x];
+            const float a = C.ax, b = C.bx;
             pvx_x = b * pp[0] + a * dvx_dx;
             pvy_x = b * pp[1] + a * dvy_dx;
             pvz_x = b * pp[2] + a * dvz_dx;
@@ -165,7 +170,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS> &
             const int ys = y < W ? y : y - (ny - 2 * W);
             const int64_t st = (int64_t)2 * W * nz * nx;
             float *p = I.psi_y + ((int64_t)ys * nz + z) * nx + x;
-            const float a = I.cpml[2 * nx + y], b = I.cpml[2 * nx + ny + y];
+            const float a = C.ay, b = C.by;
             pvy_y = b * pp[3] + a * dvy_dy;
             pvx_y = b * pp[4] + a * dvx_dy;
             pvz_y = b * pp[5] + a * dvz_dy;
@@ -177,7 +182,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS> &
             const int zs = z - (nz - W);
             const int64_t st = (int64_t)ny * W * nx;
             float *p = I.psi_z + ((int64_t)y * W + zs) * nx + x;
-            const float a = I.cpml[2 * nx + 2 * ny + z], b = I.cpml[2 * nx + 2 * ny + nz + z];
+            const float a = C.az, b = C.bz;
             pvz_z = b * pp[6] + a * dvz_dz;
             pvx_z = b * pp[7] + a * dvx_dz;
             pvy_z = b * pp[8] + a * dvy_dz;
@@ -278,12 +283,12 @@ __device__ __forceinline__ void load_psi(const EfmInst &I, int x, int y, int z, 
 }  // namespace
 
 // halo fields: vx vy vz 1/mu ; center fields: lambda txx tyy tzz txy txz tyz
-template <int PASS, int ROWS>
-__global__ void __launch_bounds__(EFM_STHREADS, ROWS == 1 ? 3 : 2)
+template <int PASS, int ROWS, int SR>
+__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
 efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     constexpr int NH = 4, NC = 7;
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t bars[EFM_SR];
+    __shared__ uint64_t bars[SR];
     __shared__ int s_src;
     __shared__ unsigned long long s_rec;
     const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
@@ -293,11 +298,14 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
-    Ring<ROWS> R{smem, bars, NH * Ring<ROWS>::HB + NC * Ring<ROWS>::CB, NH, T.ys - 1};
-    stream_setup<ROWS, NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
+    stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const bool has_src = s_src != 0;
     bool colin[ROWS];
     int hidx[ROWS], cidx[ROWS];
+    Coef cf[ROWS];
+    const bool xpml = x < nx && (x < W || x >= nx - W);
+    const float cx_a = xpml ? I.cpml[x] : 0.f, cx_b = xpml ? I.cpml[nx + x] : 0.f;
 #pragma unroll
     for (int h = 0; h < ROWS; ++h) {
         const int lz = lr + 4 * h, z = T.z0 + lz;
@@ -305,9 +313,14 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         cidx[h] = lz * EFM_STX + lx;
         colin[h] = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS &&
                    !(PASS == EFM_REV && (x < W || x >= nx - W || z >= nz - W));
+        const bool zpml = z < nz && z >= nz - W;
+        cf[h].ax = cx_a;
+        cf[h].bx = cx_b;
+        cf[h].az = zpml ? I.cpml[2 * nx + 2 * ny + z] : 0.f;
+        cf[h].bz = zpml ? I.cpml[2 * nx + 2 * ny + nz + z] : 0.f;
     }
     const int last = T.ye;
-    int issued_hi = min(last, R.p0 + EFM_SR - 1);
+    int issued_hi = min(last, R.p0 + SR - 1);
     bool ok;
     {
         const bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), I.err) &&
@@ -316,6 +329,13 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     }
     for (int j = T.ys; j < T.ye && ok; ++j) {
         const bool plane_in = j >= EFM_HS && j < ny - EFM_HS && !(PASS == EFM_REV && (j < W || j >= ny - W));
+        const bool ypml = j < W || j >= ny - W;
+        const float cy_a = ypml ? I.cpml[2 * nx + j] : 0.f, cy_b = ypml ? I.cpml[2 * nx + ny + j] : 0.f;
+#pragma unroll
+        for (int h = 0; h < ROWS; ++h) {
+            cf[h].ay = cy_a;
+            cf[h].by = cy_b;
+        }
         float pp[ROWS][9];
         if (PASS != EFM_REV) {
 #pragma unroll
@@ -328,26 +348,26 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
 #pragma unroll
             for (int h = 0; h < ROWS; ++h)
                 if (colin[h])
-                    stress_cell<PASS, ROWS>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, hidx[h],
-                                      cidx[h], has_src, pp[h]);
+                    stress_cell<PASS, ROWS, SR>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, hidx[h],
+                                      cidx[h], has_src, pp[h], cf[h]);
         }
         ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
         if (!ok) break;
-        if (j - 1 + EFM_SR <= last) {
-            if (threadIdx.x == 0) issue_plane<ROWS, NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
-            issued_hi = j - 1 + EFM_SR;
+        if (j - 1 + SR <= last) {
+            if (threadIdx.x == 0) issue_plane<ROWS, SR, NH, NC>(R, tm, T.x0, T.z0, j - 1 + SR);
+            issued_hi = j - 1 + SR;
         }
     }
     if (!ok) drain(R, R.p0, issued_hi);  // no load may still target this block's smem
 }
 
 // halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint)
-template <int PASS, int ROWS>
-__global__ void __launch_bounds__(EFM_STHREADS, ROWS == 1 ? 3 : 2)
+template <int PASS, int ROWS, int SR>
+__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
 efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     constexpr int NH = 6, NC = 4;
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t bars[EFM_SR];
+    __shared__ uint64_t bars[SR];
     __shared__ int s_src;
     __shared__ unsigned long long s_rec;
     const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
@@ -357,11 +377,14 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
-    Ring<ROWS> R{smem, bars, NH * Ring<ROWS>::HB + NC * Ring<ROWS>::CB, NH, T.ys - 1};
-    stream_setup<ROWS, NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
+    stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const unsigned long long recbits = s_rec;
     bool colin[ROWS], colgrid[ROWS];
     int hidx[ROWS], cidx[ROWS];
+    float cz_a[ROWS], cz_b[ROWS];
+    const bool xpml = x < nx && (x < W || x >= nx - W);
+    const float cx_a = xpml ? I.cpml[x] : 0.f, cx_b = xpml ? I.cpml[nx + x] : 0.f;
 #pragma unroll
     for (int h = 0; h < ROWS; ++h) {
         const int lz = lr + 4 * h, z = T.z0 + lz;
@@ -369,9 +392,12 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         cidx[h] = lz * EFM_STX + lx;
         colin[h] = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS;
         colgrid[h] = x < nx && z < nz;
+        const bool zpml = z < nz && z >= nz - W;
+        cz_a[h] = zpml ? I.cpml[2 * nx + 2 * ny + z] : 0.f;
+        cz_b[h] = zpml ? I.cpml[2 * nx + 2 * ny + nz + z] : 0.f;
     }
     const int last = T.ye;
-    int issued_hi = min(last, R.p0 + EFM_SR - 1);
+    int issued_hi = min(last, R.p0 + SR - 1);
     bool ok;
     {
         bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), I.err) &&
@@ -383,6 +409,8 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         const int y = j;
         const bool plane_in = j >= EFM_HS && j < ny - EFM_HS;
         const bool rec_plane = (recbits >> (j - T.ys)) & 1ull;
+        const bool ypml = j < W || j >= ny - W;
+        const float cy_a = ypml ? I.cpml[2 * nx + j] : 0.f, cy_b = ypml ? I.cpml[2 * nx + ny + j] : 0.f;
         float pp[ROWS][9];
         if (PASS != EFM_REV) {
 #pragma unroll
@@ -470,7 +498,7 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
                         const int xs = x < W ? x : x - (nx - 2 * W);
                         const int64_t st = (int64_t)ny * nz * 2 * W;
                         float *p = I.psi_x + 3 * st + ((int64_t)y * nz + z) * (2 * W) + xs;
-                        const float a = I.cpml[x], b = I.cpml[nx + x];
+                        const float a = cx_a, b = cx_b;
                         q1 = b * p9[0] + a * dtxx_dx;
                         q2 = b * p9[1] + a * dtxy_dx;
                         q3 = b * p9[2] + a * dtxz_dx;
@@ -482,7 +510,7 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
                         const int ys = y < W ? y : y - (ny - 2 * W);
                         const int64_t st = (int64_t)2 * W * nz * nx;
                         float *p = I.psi_y + 3 * st + ((int64_t)ys * nz + z) * nx + x;
-                        const float a = I.cpml[2 * nx + y], b = I.cpml[2 * nx + ny + y];
+                        const float a = cy_a, b = cy_b;
                         q4 = b * p9[3] + a * dtyy_dy;
                         q5 = b * p9[4] + a * dtxy_dy;
                         q6 = b * p9[5] + a * dtyz_dy;
@@ -494,7 +522,7 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
                         const int zs = z - (nz - W);
                         const int64_t st = (int64_t)ny * W * nx;
                         float *p = I.psi_z + 3 * st + ((int64_t)y * W + zs) * nx + x;
-                        const float a = I.cpml[2 * nx + 2 * ny + z], b = I.cpml[2 * nx + 2 * ny + nz + z];
+                        const float a = cz_a[h], b = cz_b[h];
                         q7 = b * p9[6] + a * dtzz_dz;
                         q8 = b * p9[7] + a * dtxz_dz;
                         q9 = b * p9[8] + a * dtyz_dz;
@@ -551,9 +579,9 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         }
         ok = __syncthreads_and(mine) != 0;
         if (!ok) break;
-        if (j - 1 + EFM_SR <= last) {
-            if (threadIdx.x == 0) issue_plane<ROWS, NH, NC>(R, tm, T.x0, T.z0, j - 1 + EFM_SR);
-            issued_hi = j - 1 + EFM_SR;
+        if (j - 1 + SR <= last) {
+            if (threadIdx.x == 0) issue_plane<ROWS, SR, NH, NC>(R, tm, T.x0, T.z0, j - 1 + SR);
+            issued_hi = j - 1 + SR;
         }
     }
     if (!ok) drain(R, R.p0, issued_hi);
@@ -572,37 +600,41 @@ __global__ void efm_model_reciprocals(const float *__restrict__ mu, const float 
 cudaError_t efm_image_init_attributes();
 
 // ---------------------------------------------------------------------------- launchers
-template <int ROWS>
-constexpr int kSmemStress = efm_stream_smem(ROWS, 4, 7);
-template <int ROWS>
-constexpr int kSmemVelocity = efm_stream_smem(ROWS, 6, 4);
+template <int ROWS, int SR>
+constexpr int kSmemStress = efm_stream_smem(ROWS, SR, 4, 7);
+template <int ROWS, int SR>
+constexpr int kSmemVelocity = efm_stream_smem(ROWS, SR, 6, 4);
 
-template <int ROWS>
+template <int ROWS, int SR>
 static void launch_rows(int pass, int kind, const EfmInst *insts, int ninst, int tiles, int it,
                         cudaStream_t s) {
+    constexpr int SS = kSmemStress<ROWS, SR>, SV = kSmemVelocity<ROWS, SR>;
     if (kind == 0) {
         switch (pass) {
-            case EFM_FWD: efm_stress_stream<EFM_FWD, ROWS><<<tiles, EFM_STHREADS, kSmemStress<ROWS>, s>>>(insts, ninst, it); break;
-            case EFM_ADJ: efm_stress_stream<EFM_ADJ, ROWS><<<tiles, EFM_STHREADS, kSmemStress<ROWS>, s>>>(insts, ninst, it); break;
-            default: efm_stress_stream<EFM_REV, ROWS><<<tiles, EFM_STHREADS, kSmemStress<ROWS>, s>>>(insts, ninst, it); break;
+            case EFM_FWD: efm_stress_stream<EFM_FWD, ROWS, SR><<<tiles, EFM_STHREADS, SS, s>>>(insts, ninst, it); break;
+            case EFM_ADJ: efm_stress_stream<EFM_ADJ, ROWS, SR><<<tiles, EFM_STHREADS, SS, s>>>(insts, ninst, it); break;
+            default: efm_stress_stream<EFM_REV, ROWS, SR><<<tiles, EFM_STHREADS, SS, s>>>(insts, ninst, it); break;
         }
     } else {
         switch (pass) {
-            case EFM_FWD: efm_velocity_stream<EFM_FWD, ROWS><<<tiles, EFM_STHREADS, kSmemVelocity<ROWS>, s>>>(insts, ninst, it); break;
-            case EFM_ADJ: efm_velocity_stream<EFM_ADJ, ROWS><<<tiles, EFM_STHREADS, kSmemVelocity<ROWS>, s>>>(insts, ninst, it); break;
-            default: efm_velocity_stream<EFM_REV, ROWS><<<tiles, EFM_STHREADS, kSmemVelocity<ROWS>, s>>>(insts, ninst, it); break;
+            case EFM_FWD: efm_velocity_stream<EFM_FWD, ROWS, SR><<<tiles, EFM_STHREADS, SV, s>>>(insts, ninst, it); break;
+            case EFM_ADJ: efm_velocity_stream<EFM_ADJ, ROWS, SR><<<tiles, EFM_STHREADS, SV, s>>>(insts, ninst, it); break;
+            default: efm_velocity_stream<EFM_REV, ROWS, SR><<<tiles, EFM_STHREADS, SV, s>>>(insts, ninst, it); break;
         }
     }
 }
 
-// kind 0 = stress, 1 = velocity; rows = cells per thread (1 or 2), matching the tile layout
-// and tensor-map boxes the table was built with.
-extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, const EfmInst *insts,
-                                         int ninst, int tiles, int it, cudaStream_t s) {
-    if (rows == 1)
-        launch_rows<1>(pass, kind, insts, ninst, tiles, it, s);
+// kind 0 = stress, 1 = velocity; rows = cells per thread (1 or 2) and ring = stages (4, or
+// 6 with one row), matching the tile layout and tensor-map boxes the table was built with.
+extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, int ring,
+                                         const EfmInst *insts, int ninst, int tiles, int it,
+                                         cudaStream_t s) {
+    if (rows == 1 && ring == 6)
+        launch_rows<1, 6>(pass, kind, insts, ninst, tiles, it, s);
+    else if (rows == 1)
+        launch_rows<1, 4>(pass, kind, insts, ninst, tiles, it, s);
     else
-        launch_rows<2>(pass, kind, insts, ninst, tiles, it, s);
+        launch_rows<2, 4>(pass, kind, insts, ninst, tiles, it, s);
     return cudaGetLastError();
 }
 
@@ -614,22 +646,23 @@ extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho,
     return cudaGetLastError();
 }
 
-template <int ROWS>
+template <int ROWS, int SR>
 static cudaError_t set_rows_attributes() {
     cudaError_t e;
-    const int ss = kSmemStress<ROWS>, sv = kSmemVelocity<ROWS>;
+    const int ss = kSmemStress<ROWS, SR>, sv = kSmemVelocity<ROWS, SR>;
     const auto A = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_FWD, ROWS>, A, ss))) return e;
-    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_ADJ, ROWS>, A, ss))) return e;
-    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_REV, ROWS>, A, ss))) return e;
-    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD, ROWS>, A, sv))) return e;
-    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ, ROWS>, A, sv))) return e;
-    return cudaFuncSetAttribute(efm_velocity_stream<EFM_REV, ROWS>, A, sv);
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_FWD, ROWS, SR>, A, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_ADJ, ROWS, SR>, A, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_REV, ROWS, SR>, A, ss))) return e;
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD, ROWS, SR>, A, sv))) return e;
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ, ROWS, SR>, A, sv))) return e;
+    return cudaFuncSetAttribute(efm_velocity_stream<EFM_REV, ROWS, SR>, A, sv);
 }
 
 extern "C" cudaError_t efm_stream_init_attributes() {
     cudaError_t e;
-    if ((e = set_rows_attributes<1>())) return e;
-    if ((e = set_rows_attributes<2>())) return e;
+    if ((e = set_rows_attributes<1, 4>())) return e;
+    if ((e = set_rows_attributes<1, 6>())) return e;
+    if ((e = set_rows_attributes<2, 4>())) return e;
     return efm_image_init_attributes();
 }

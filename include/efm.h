@@ -192,6 +192,9 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 /* Cells per thread of the plane-streaming stress/velocity kernels: 2 (64 x 8 tiles, two
  * blocks per SM) or 1 (64 x 4 tiles, three blocks per SM); 0 (default) = 2. */
 #define EFM_OPT_TILE_ROWS 4
+/* Shared-memory ring depth of the plane-streaming kernels: 4 (default) or 6 (with one-row
+ * tiles only: four planes in flight per block, two blocks per SM); 0 = 4. */
+#define EFM_OPT_RING_DEPTH 5
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*

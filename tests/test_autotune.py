@@ -26,11 +26,12 @@ def test_cache_roundtrip_and_key_order(tmp_path):
     assert autotune.load_cache(p) == {}
 
 
-def test_candidates_cover_both_tile_heights():
+def test_candidates_cover_both_tile_heights_and_ring_depths():
     from elastic_fm_vp_vs_rho_b200 import autotune
-    rows = {r for r, _ in autotune.DEFAULT_CANDIDATES}
-    assert rows == {1, 2}
-    assert all(0 <= yc <= 64 for _, yc in autotune.DEFAULT_CANDIDATES)
+    rows = {r for r, _, _ in autotune.DEFAULT_CANDIDATES}
+    rings = {(r, d) for r, d, _ in autotune.DEFAULT_CANDIDATES}
+    assert rows == {1, 2} and (1, 6) in rings and (2, 6) not in rings
+    assert all(0 <= yc <= 64 for _, _, yc in autotune.DEFAULT_CANDIDATES)
 
 
 @pytest.mark.gpu
@@ -46,7 +47,7 @@ def test_tune_applies_a_choice_and_reuses_the_cache(golden_c1scale, cuda, tmp_pa
     ref = b.forward().cpu().numpy()
     p = str(tmp_path / "tune.json")
     c1 = autotune.tune(b, nt_probe=12, path=p, repeats=1,
-                       candidates=((2, 0), (1, 0), (1, 8)))
+                       candidates=((2, 4, 0), (1, 4, 0), (1, 6, 8)))
     assert not c1["cached"] and c1["rows"] in (1, 2) and os.path.exists(p)
     got = b.forward().cpu().numpy()
     assert rel_err(got, ref) < 1e-5  # any launch shape computes the same gathers

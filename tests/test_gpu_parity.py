@@ -291,8 +291,9 @@ def test_receivers_on_never_updated_cells(golden_c1scale, cuda):
     assert rel_err(m[0, 0].cpu().numpy(), gm) < TOL_MT
 
 
-@pytest.mark.parametrize("ychunk,rows", [(0, 2), (5, 2), (64, 2), (0, 1), (7, 1)])
-def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychunk, rows):
+@pytest.mark.parametrize("ychunk,rows,ring", [(0, 2, 4), (5, 2, 4), (64, 2, 4), (0, 1, 4), (7, 1, 4),
+                                              (0, 1, 6), (3, 1, 6)])
+def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychunk, rows, ring):
     """TMA plane-streaming kernels = one-thread-per-cell kernels (same arithmetic up to the
     hardware reciprocal in the harmonic means), for the forward, the adjoint, the reverse
     rebuild and the MT gradient; several chunk lengths and both tile heights (64 x 8 tiles
@@ -305,6 +306,7 @@ def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychu
         b.set_option(_lib.EFM_OPT_STREAM_KERNELS, stream)
         b.set_option(_lib.EFM_OPT_YCHUNK, ychunk)
         b.set_option(_lib.EFM_OPT_TILE_ROWS, rows)
+        b.set_option(_lib.EFM_OPT_RING_DEPTH, ring)
         mod = b.forward(save_borders=True)
         res, _ = b.residual_misfit(mod, cuda.as_tensor(d["obs0"].reshape(-1)).cuda())
         g, m = b.gradient(res, model=True, mt=True)

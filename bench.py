@@ -101,7 +101,7 @@ def algorithmic_bytes(w):
     pml_dirs = ny * nz * 2 * W + 2 * W * nz * nx + ny * W * nx  # sum over cells of #directions
     box = (nx - 2 * W) * (ny - 2 * W) * (nz - W)
     ntr = 3 * w.nt * len(w.shots[0].rec_x)
-    return {
+    b = {
         "fwd_stress": 68 * n + 24 * pml_dirs,
         "fwd_velocity": 52 * n + 24 * pml_dirs,
         "adj_stress": 68 * n + 24 * pml_dirs,
@@ -112,6 +112,10 @@ def algorithmic_bytes(w):
         "residual_misfit": 12 * ntr,
         "model_reciprocals": 16 * n,
     }
+    # paired launches of the gradient (both half-steps in one grid)
+    b["adj_stress+rev_velocity"] = b["adj_stress"] + b["rev_velocity"]
+    b["rev_stress+adj_velocity"] = b["rev_stress"] + b["adj_velocity"]
+    return b
 
 
 # ----------------------------------------------------------------------------- clocks

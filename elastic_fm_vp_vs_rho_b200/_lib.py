@@ -30,9 +30,11 @@ EFM_SAVE_CHECKPOINTS = 2
 EFM_OPT_CHECKPOINT_EVERY = 3
 EFM_OPT_TILE_ROWS = 4
 EFM_OPT_RING_DEPTH = 5
-EFM_NKERN = 9
+EFM_OPT_PAIR_LAUNCH = 6
+EFM_NKERN = 11
 KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity",
-                "rev_stress", "residual_misfit", "model_reciprocals", "imaging")
+                "rev_stress", "residual_misfit", "model_reciprocals", "imaging",
+                "adj_stress+rev_velocity", "rev_stress+adj_velocity")
 
 _ERRNAMES = {EFM_ERR_ARG: "EFM_ERR_ARG", EFM_ERR_CUDA: "EFM_ERR_CUDA",
              EFM_ERR_STATE: "EFM_ERR_STATE", EFM_ERR_NOMEM: "EFM_ERR_NOMEM",

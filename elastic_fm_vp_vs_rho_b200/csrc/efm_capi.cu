@@ -26,6 +26,9 @@ extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, int ring,
                                          const EfmInst *insts, int ninst, int tiles, int it,
                                          cudaStream_t s);
 extern "C" cudaError_t efm_stream_init_attributes();
+extern "C" cudaError_t efm_launch_pair(int which, int rows, int ring, const EfmInst *ts,
+                                       int tiles_s, const EfmInst *tv, int tiles_v, int ninst,
+                                       int it, cudaStream_t s);
 extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int tiles, int it,
                                         cudaStream_t s);
 extern "C" cudaError_t efm_launch_exact(int kind, const EfmExact *t, int n, int tiles, int step,
@@ -145,6 +148,7 @@ struct efm_ctx {
     int opt_ychunk = 0;
     int opt_rows = 0;
     int opt_ring = 0;
+    int opt_pair = 1;
     int rows = 2;  // cells per thread of the tables last built for the streaming kernels
     int ring = 4;  // ring depth of those tables' kernels
     int opt_ck_every = 50;
@@ -1087,6 +1091,29 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                 return rc;
     auto dtab = [&](int k) { return (const EfmInst *)(ctx->d_tab + (size_t)k * n); };
     for (int it = 0; it < maxsteps; ++it) {
+        if (st && model && ctx->opt_pair) {
+            // (adjoint stress | rebuild velocity), (rebuild stress | adjoint velocity), imaging:
+            // within a step the adjoint chain and the rebuild write disjoint fields, and the
+            // imaging reads neither the rebuild's stress nor anything the next step's first
+            // pair writes before this step's imaging has finished (stream order)
+            const int kv = (it & 1) ? T_REV_V1 : T_REV_V0, ks = (it & 1) ? T_REV_S1 : T_REV_S0;
+            const int ki = (it & 1) ? T_IMG1 : T_IMG0;
+            if ((rc = timed_launch(ctx, EFM_K_PAIR_ADJS_REVV, s, [&] {
+                     return efm_launch_pair(0, ctx->rows, ctx->ring, dtab(T_ADJ_S), ctx->tiles[T_ADJ_S],
+                                            dtab(kv), ctx->tiles[kv], n, it, s);
+                 })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_PAIR_REVS_ADJV, s, [&] {
+                     return efm_launch_pair(1, ctx->rows, ctx->ring, dtab(ks), ctx->tiles[ks],
+                                            dtab(T_ADJ_V), ctx->tiles[T_ADJ_V], n, it, s);
+                 })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_IMAGING, s, [&] {
+                     return efm_launch_image(dtab(ki), n, ctx->tiles[ki], it, s);
+                 })))
+                return rc;
+            continue;
+        }
         if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
                  return st ? efm_launch_stream(EFM_ADJ, 0, ctx->rows, ctx->ring, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
                            : efm_launch_stress(EFM_ADJ, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s);
@@ -1139,6 +1166,7 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             if (value < 0 || value > 2) return fail(EFM_ERR_ARG, "tile rows must be 0, 1 or 2");
             ctx->opt_rows = value;
             break;
+        case EFM_OPT_PAIR_LAUNCH: ctx->opt_pair = value != 0; break;
         case EFM_OPT_RING_DEPTH:
             if (value != 0 && value != 4 && value != 6) return fail(EFM_ERR_ARG, "ring depth must be 0, 4 or 6");
             ctx->opt_ring = value;

@@ -284,16 +284,15 @@ __device__ __forceinline__ void load_psi(const EfmInst &I, int x, int y, int z, 
 
 // halo fields: vx vy vz 1/mu ; center fields: lambda txx tyy tzz txy txz tyz
 template <int PASS, int ROWS, int SR>
-__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
-efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
+__device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, int ninst, int it,
+                                            int block, unsigned char *smem) {
     constexpr int NH = 4, NC = 7;
-    extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint64_t bars[SR];
     __shared__ int s_src;
     __shared__ unsigned long long s_rec;
-    const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
+    const EfmInst &I = insts[efm_find_inst(insts, ninst, block)];
     if (it >= I.nsteps) return;
-    const Tile T = stream_tile<ROWS>(I, blockIdx.x);
+    const Tile T = stream_tile<ROWS>(I, block);
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
@@ -363,16 +362,15 @@ efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
 
 // halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint)
 template <int PASS, int ROWS, int SR>
-__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
-efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
+__device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts, int ninst, int it,
+                                              int block, unsigned char *smem) {
     constexpr int NH = 6, NC = 4;
-    extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint64_t bars[SR];
     __shared__ int s_src;
     __shared__ unsigned long long s_rec;
-    const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
+    const EfmInst &I = insts[efm_find_inst(insts, ninst, block)];
     if (it >= I.nsteps) return;
-    const Tile T = stream_tile<ROWS>(I, blockIdx.x);
+    const Tile T = stream_tile<ROWS>(I, block);
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
@@ -587,6 +585,36 @@ efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     if (!ok) drain(R, R.p0, issued_hi);
 }
 
+template <int PASS, int ROWS, int SR>
+__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
+efm_stress_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    stress_body<PASS, ROWS, SR>(insts, ninst, it, blockIdx.x, smem);
+}
+
+template <int PASS, int ROWS, int SR>
+__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
+efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    velocity_body<PASS, ROWS, SR>(insts, ninst, it, blockIdx.x, smem);
+}
+
+// Two independent half-steps in one launch: blocks [0, tiles_s) run the stress pass PS of
+// table ts, the rest the velocity pass PV of table tv.  The gradient's adjoint chain and its
+// reverse-time rebuild touch disjoint fields within a step, so (adjoint stress, rebuild
+// velocity) and (rebuild stress, adjoint velocity) can share a grid and fill the SMs
+// together instead of running back to back.
+template <int PS, int PV, int ROWS, int SR>
+__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
+efm_pair_stream(const EfmInst *__restrict__ ts, int tiles_s, const EfmInst *__restrict__ tv,
+                int ninst, int it) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    if ((int)blockIdx.x < tiles_s)
+        stress_body<PS, ROWS, SR>(ts, ninst, it, blockIdx.x, smem);
+    else
+        velocity_body<PV, ROWS, SR>(tv, ninst, it, blockIdx.x - tiles_s, smem);
+}
+
 // 1/mu and 1/rho for the streaming kernels (once per call; the model may change in place).
 __global__ void efm_model_reciprocals(const float *__restrict__ mu, const float *__restrict__ rho,
                                       float *__restrict__ rmu, float *__restrict__ buoy, int64_t n) {
@@ -624,6 +652,31 @@ static void launch_rows(int pass, int kind, const EfmInst *insts, int ninst, int
     }
 }
 
+template <int ROWS, int SR>
+static void launch_pair_rows(int which, const EfmInst *ts, int tiles_s, const EfmInst *tv,
+                             int tiles_v, int ninst, int it, cudaStream_t s) {
+    constexpr int SM = kSmemStress<ROWS, SR> > kSmemVelocity<ROWS, SR> ? kSmemStress<ROWS, SR>
+                                                                       : kSmemVelocity<ROWS, SR>;
+    if (which == 0)
+        efm_pair_stream<EFM_ADJ, EFM_REV, ROWS, SR><<<tiles_s + tiles_v, EFM_STHREADS, SM, s>>>(ts, tiles_s, tv, ninst, it);
+    else
+        efm_pair_stream<EFM_REV, EFM_ADJ, ROWS, SR><<<tiles_s + tiles_v, EFM_STHREADS, SM, s>>>(ts, tiles_s, tv, ninst, it);
+}
+
+// which 0: adjoint stress (ts) + rebuild velocity (tv); 1: rebuild stress (ts) + adjoint
+// velocity (tv).
+extern "C" cudaError_t efm_launch_pair(int which, int rows, int ring, const EfmInst *ts,
+                                       int tiles_s, const EfmInst *tv, int tiles_v, int ninst,
+                                       int it, cudaStream_t s) {
+    if (rows == 1 && ring == 6)
+        launch_pair_rows<1, 6>(which, ts, tiles_s, tv, tiles_v, ninst, it, s);
+    else if (rows == 1)
+        launch_pair_rows<1, 4>(which, ts, tiles_s, tv, tiles_v, ninst, it, s);
+    else
+        launch_pair_rows<2, 4>(which, ts, tiles_s, tv, tiles_v, ninst, it, s);
+    return cudaGetLastError();
+}
+
 // kind 0 = stress, 1 = velocity; rows = cells per thread (1 or 2) and ring = stages (4, or
 // 6 with one row), matching the tile layout and tensor-map boxes the table was built with.
 extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, int ring,
@@ -656,7 +709,10 @@ static cudaError_t set_rows_attributes() {
     if ((e = cudaFuncSetAttribute(efm_stress_stream<EFM_REV, ROWS, SR>, A, ss))) return e;
     if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD, ROWS, SR>, A, sv))) return e;
     if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ, ROWS, SR>, A, sv))) return e;
-    return cudaFuncSetAttribute(efm_velocity_stream<EFM_REV, ROWS, SR>, A, sv);
+    if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_REV, ROWS, SR>, A, sv))) return e;
+    const int sp = ss > sv ? ss : sv;
+    if ((e = cudaFuncSetAttribute(efm_pair_stream<EFM_ADJ, EFM_REV, ROWS, SR>, A, sp))) return e;
+    return cudaFuncSetAttribute(efm_pair_stream<EFM_REV, EFM_ADJ, ROWS, SR>, A, sp);
 }
 
 extern "C" cudaError_t efm_stream_init_attributes() {

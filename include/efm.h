@@ -195,6 +195,9 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 /* Shared-memory ring depth of the plane-streaming kernels: 4 (default) or 6 (with one-row
  * tiles only: four planes in flight per block, two blocks per SM); 0 = 4. */
 #define EFM_OPT_RING_DEPTH 5
+/* 1 (default): in the imaging gradient, launch the adjoint and rebuild half-steps of a
+ * time step pairwise in one grid (they touch disjoint fields); 0: five launches per step. */
+#define EFM_OPT_PAIR_LAUNCH 6
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*
@@ -215,7 +218,9 @@ EFM_API int efm_status(efm_ctx *ctx, void *stream);
 #define EFM_K_REDUCE 6         /* residual + misfit reduction */
 #define EFM_K_MODEL_AUX 7      /* 1/mu, 1/rho for the plane-streaming kernels (once per call) */
 #define EFM_K_IMAGING 8        /* zero-lag imaging (plane-streaming kernels) */
-#define EFM_NKERN 9
+#define EFM_K_PAIR_ADJS_REVV 9 /* adjoint stress + rebuild velocity in one launch */
+#define EFM_K_PAIR_REVS_ADJV 10 /* rebuild stress + adjoint velocity in one launch */
+#define EFM_NKERN 11
 
 /*
  * Record a CUDA event pair around every kernel launch of this context (enable = 1) so that

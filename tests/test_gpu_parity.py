@@ -317,3 +317,24 @@ def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychu
     for i in range(3):
         assert rel_err(g1[i], g2[i]) < 5e-5
     assert rel_err(t1, t2) < 2e-5
+
+
+@pytest.mark.parametrize("rows,ring", [(2, 4), (1, 4), (1, 6)])
+def test_paired_gradient_launches_equal_sequential(golden_c1scale, cuda, rows, ring):
+    """The gradient's adjoint / rebuild half-steps launched pairwise in one grid give
+    bit-identical gradients to five launches per step."""
+    from elastic_fm_vp_vs_rho_b200 import _lib
+    d = golden_c1scale
+    out = []
+    for pair in (1, 0):
+        b = _batch(d, d["lam0"], d["mu0"], d["rho0"], d["mt_obs"])
+        b.set_option(_lib.EFM_OPT_TILE_ROWS, rows)
+        b.set_option(_lib.EFM_OPT_RING_DEPTH, ring)
+        b.set_option(_lib.EFM_OPT_PAIR_LAUNCH, pair)
+        mod = b.forward(save_borders=True)
+        res, _ = b.residual_misfit(mod, cuda.as_tensor(d["obs0"].reshape(-1)).cuda())
+        g, m = b.gradient(res, model=True, mt=True)
+        b.status()
+        out.append((g.cpu().numpy(), m.cpu().numpy()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])

@@ -260,6 +260,17 @@ void layout_stream(EfmInst &d, int ychunk, int tz) {
     d.tiles_y = (d.ny + ychunk - 1) / ychunk;
 }
 
+// The streaming kernels address the fields of a pass from its first volume (consecutive
+// volumes of one allocation); every table they run on must keep that layout.
+bool fields_contiguous(const EfmInst &d) {
+    const int64_t nc = (int64_t)d.nx * d.ny * d.nz;
+    for (int k = 1; k < 6; ++k)
+        if (d.f.t[k] != d.f.t[0] + k * nc) return false;
+    for (int c = 1; c < 3; ++c)
+        if (d.f.v[c] != d.f.v[0] + c * nc || d.f.vo[c] != d.f.vo[0] + c * nc) return false;
+    return true;
+}
+
 // prefix tile offsets of one table; returns its total tile count
 int finish_table(EfmInst *t, int n) {
     int tiles = 0;
@@ -552,6 +563,9 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
         tab[i] = ds;
         tab[(size_t)n + i] = dv;
     }
+    if (st)
+        for (const EfmInst &e : tab)
+            if (!fields_contiguous(e)) return fail(EFM_ERR_STATE, "field volumes not contiguous");
     ctx->tiles[T_FWD_S] = finish_table(tab.data(), n);
     ctx->tiles[T_FWD_V] = finish_table(tab.data() + n, n);
     if (st)
@@ -1077,6 +1091,9 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
             slot(p == 0 ? T_IMG0 : T_IMG1, i) = ri;
         }
     }
+    if (st)
+        for (const EfmInst &e : tab)
+            if (!fields_contiguous(e)) return fail(EFM_ERR_STATE, "field volumes not contiguous");
     for (int k = T_ADJ_S; k < T_NSLOT; ++k) ctx->tiles[k] = finish_table(&slot(k, 0), n);
     if (st)
         EFM_CK(cudaMemcpyAsync(ctx->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),

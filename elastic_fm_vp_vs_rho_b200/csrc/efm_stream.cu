@@ -133,10 +133,33 @@ struct Coef {
     float ax, bx, ay, by, az, bz;
 };
 
+// Per-block constants of the plane loop, read from the instance table once.  The loop's
+// mbarrier waits are asm statements with a memory clobber, after which the compiler would
+// otherwise reload every table field it touches; the fields of a pass are consecutive
+// volumes of one allocation, so one base pointer and the volume size address all of them.
+struct Hot {
+    float *out;       // first output volume: txx (stress) or vx (velocity / rebuild target)
+    float *psx, *psy, *psz;
+    int64_t nc;       // cells per volume
+    float k;
+};
+
+__device__ __forceinline__ Hot make_hot(const EfmInst &I, float *out) {
+    Hot h;
+    h.out = out;
+    h.psx = I.psi_x;
+    h.psy = I.psi_y;
+    h.psz = I.psi_z;
+    h.nc = (int64_t)I.nx * I.ny * I.nz;
+    h.k = I.k;
+    return h;
+}
+
 template <int PASS, int ROWS, int SR>
 __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, SR> &R, int sm, int s0,
                                             int sp, int it, int x, int y, int z, int hidx,
-                                            int cidx, bool has_src, const float *pp, const Coef &C) {
+                                            int cidx, bool has_src, const float *pp, const Coef &C,
+                                            const Hot &H) {
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
     const float *vx0 = R.halo(s0, 0), *vy0 = R.halo(s0, 1), *vz0 = R.halo(s0, 2);
     const float *rm0 = R.halo(s0, 3), *rm1 = R.halo(sp, 3);
@@ -157,7 +180,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
         if (x < W || x >= nx - W) {
             const int xs = x < W ? x : x - (nx - 2 * W);
             const int64_t st = (int64_t)ny * nz * 2 * W;
-            float *p = I.psi_x + ((int64_t)y * nz + z) * (2 * W) + xs;
+            float *p = H.psx + ((int64_t)y * nz + z) * (2 * W) + xs;
             const float a = C.ax, b = C.bx;
             pvx_x = b * pp[0] + a * dvx_dx;
             pvy_x = b * pp[1] + a * dvy_dx;
@@ -169,7 +192,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
         if (y < W || y >= ny - W) {
             const int ys = y < W ? y : y - (ny - 2 * W);
             const int64_t st = (int64_t)2 * W * nz * nx;
-            float *p = I.psi_y + ((int64_t)ys * nz + z) * nx + x;
+            float *p = H.psy + ((int64_t)ys * nz + z) * nx + x;
             const float a = C.ay, b = C.by;
             pvy_y = b * pp[3] + a * dvy_dy;
             pvx_y = b * pp[4] + a * dvx_dy;
@@ -181,7 +204,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
         if (z >= nz - W) {
             const int zs = z - (nz - W);
             const int64_t st = (int64_t)ny * W * nx;
-            float *p = I.psi_z + ((int64_t)y * W + zs) * nx + x;
+            float *p = H.psz + ((int64_t)y * W + zs) * nx + x;
             const float a = C.az, b = C.bz;
             pvz_z = b * pp[6] + a * dvz_dz;
             pvx_z = b * pp[7] + a * dvx_dz;
@@ -200,7 +223,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
     const float mu_xy = 4.f * frcp(r0 + ri + rj + rij);
     const float mu_yz = 4.f * frcp(r0 + rj + rk + rjk);
     const float lam = R.center(s0, 0)[cidx];
-    const float k = I.k;
+    const float k = H.k;
     const float l2m = lam + 2.f * mu0;
     float txx = R.center(s0, 1)[cidx] + k * (l2m * (dvx_dx + pvx_x) + lam * (dvy_dy + dvz_dz + pvy_y + pvz_z));
     float tyy = R.center(s0, 2)[cidx] + k * (l2m * (dvy_dy + pvy_y) + lam * (dvx_dx + dvz_dz + pvx_x + pvz_z));
@@ -224,12 +247,13 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
         }
     }
     const int64_t c = x + (int64_t)nx * (z + (int64_t)nz * y);
-    I.f.t[0][c] = txx;
-    I.f.t[1][c] = tyy;
-    I.f.t[2][c] = tzz;
-    I.f.t[3][c] = txy;
-    I.f.t[4][c] = txz;
-    I.f.t[5][c] = tyz;
+    float *o = H.out + c;
+    o[0] = txx;
+    o[H.nc] = tyy;
+    o[2 * H.nc] = tzz;
+    o[3 * H.nc] = txy;
+    o[4 * H.nc] = txz;
+    o[5 * H.nc] = tyz;
     if (PASS == EFM_ADJ && has_src && I.mtg != nullptr) {
         for (int s = 0; s < I.nsrc; ++s) {
             if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s]) {
@@ -250,14 +274,15 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
 
 // Request the 9 old CPML memory variables of one cell (zeros where the cell has none).
 template <int FIRST>
-__device__ __forceinline__ void load_psi(const EfmInst &I, int x, int y, int z, float *pp) {
+__device__ __forceinline__ void load_psi(const EfmInst &I, const Hot &H, int x, int y, int z,
+                                         float *pp) {
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
 #pragma unroll
     for (int q = 0; q < 9; ++q) pp[q] = 0.f;
     if (x < W || x >= nx - W) {
         const int xs = x < W ? x : x - (nx - 2 * W);
         const int64_t st = (int64_t)ny * nz * 2 * W;
-        const float *p = I.psi_x + FIRST * st + ((int64_t)y * nz + z) * (2 * W) + xs;
+        const float *p = H.psx + FIRST * st + ((int64_t)y * nz + z) * (2 * W) + xs;
         pp[0] = p[0];
         pp[1] = p[st];
         pp[2] = p[2 * st];
@@ -265,7 +290,7 @@ __device__ __forceinline__ void load_psi(const EfmInst &I, int x, int y, int z, 
     if (y < W || y >= ny - W) {
         const int ys = y < W ? y : y - (ny - 2 * W);
         const int64_t st = (int64_t)2 * W * nz * nx;
-        const float *p = I.psi_y + FIRST * st + ((int64_t)ys * nz + z) * nx + x;
+        const float *p = H.psy + FIRST * st + ((int64_t)ys * nz + z) * nx + x;
         pp[3] = p[0];
         pp[4] = p[st];
         pp[5] = p[2 * st];
@@ -273,7 +298,7 @@ __device__ __forceinline__ void load_psi(const EfmInst &I, int x, int y, int z, 
     if (z >= nz - W) {
         const int zs = z - (nz - W);
         const int64_t st = (int64_t)ny * W * nx;
-        const float *p = I.psi_z + FIRST * st + ((int64_t)y * W + zs) * nx + x;
+        const float *p = H.psz + FIRST * st + ((int64_t)y * W + zs) * nx + x;
         pp[6] = p[0];
         pp[7] = p[st];
         pp[8] = p[2 * st];
@@ -300,6 +325,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const bool has_src = s_src != 0;
+    const Hot H = make_hot(I, I.f.t[0]);
     bool colin[ROWS];
     int hidx[ROWS], cidx[ROWS];
     Coef cf[ROWS];
@@ -339,7 +365,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
         if (PASS != EFM_REV) {
 #pragma unroll
             for (int h = 0; h < ROWS; ++h)
-                if (plane_in && colin[h]) load_psi<0>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
+                if (plane_in && colin[h]) load_psi<0>(I, H, x, j, T.z0 + lr + 4 * h, pp[h]);
         }
         const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
         if (mine && plane_in) {
@@ -348,7 +374,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
             for (int h = 0; h < ROWS; ++h)
                 if (colin[h])
                     stress_cell<PASS, ROWS, SR>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, hidx[h],
-                                      cidx[h], has_src, pp[h], cf[h]);
+                                      cidx[h], has_src, pp[h], cf[h], H);
         }
         ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
         if (!ok) break;
@@ -378,6 +404,9 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const unsigned long long recbits = s_rec;
+    const Hot H = make_hot(I, PASS == EFM_REV ? I.f.vo[0] : I.f.v[0]);
+    float *const border = I.border;
+    const int64_t strip_n = I.strip_n;
     bool colin[ROWS], colgrid[ROWS];
     int hidx[ROWS], cidx[ROWS];
     float cz_a[ROWS], cz_b[ROWS];
@@ -413,7 +442,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
         if (PASS != EFM_REV) {
 #pragma unroll
             for (int h = 0; h < ROWS; ++h)
-                if (plane_in && colin[h]) load_psi<3>(I, x, j, T.z0 + lr + 4 * h, pp[h]);
+                if (plane_in && colin[h]) load_psi<3>(I, H, x, j, T.z0 + lr + 4 * h, pp[h]);
         }
         const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
         if (mine && PASS == EFM_REV) {
@@ -432,10 +461,10 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                 int64_t slot[3];
                 const int nslot = zone ? 0 : efm_strip_slots(I, x, y, z, slot);
                 if (nslot > 0) {
-                    const float *sv = I.border + (int64_t)(I.nt - 2 - it) * 3 * I.strip_n;
+                    const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
                     nvx = sv[slot[0]];
-                    nvy = sv[I.strip_n + slot[0]];
-                    nvz = sv[2 * I.strip_n + slot[0]];
+                    nvy = sv[strip_n + slot[0]];
+                    nvz = sv[2 * strip_n + slot[0]];
                 } else if (!zone && plane_in && colin[h]) {
                     const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
                     const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
@@ -454,14 +483,14 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
                     const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
                     const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
-                    const float k = I.k;
+                    const float k = H.k;
                     nvx = R.center(s0, 1)[ci] + k * b_x * (dtxx_dx + dtxy_dy + dtxz_dz);
                     nvy = R.center(s0, 2)[ci] + k * b_y * (dtxy_dx + dtyy_dy + dtyz_dz);
                     nvz = R.center(s0, 3)[ci] + k * b_z * (dtxz_dx + dtyz_dy + dtzz_dz);
                 }
-                I.f.vo[0][c] = nvx;
-                I.f.vo[1][c] = nvy;
-                I.f.vo[2][c] = nvz;
+                H.out[c] = nvx;
+                H.out[H.nc + c] = nvy;
+                H.out[2 * H.nc + c] = nvz;
             }
         } else if (mine) {
             const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
@@ -495,7 +524,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     if (x < W || x >= nx - W) {
                         const int xs = x < W ? x : x - (nx - 2 * W);
                         const int64_t st = (int64_t)ny * nz * 2 * W;
-                        float *p = I.psi_x + 3 * st + ((int64_t)y * nz + z) * (2 * W) + xs;
+                        float *p = H.psx + 3 * st + ((int64_t)y * nz + z) * (2 * W) + xs;
                         const float a = cx_a, b = cx_b;
                         q1 = b * p9[0] + a * dtxx_dx;
                         q2 = b * p9[1] + a * dtxy_dx;
@@ -507,7 +536,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     if (y < W || y >= ny - W) {
                         const int ys = y < W ? y : y - (ny - 2 * W);
                         const int64_t st = (int64_t)2 * W * nz * nx;
-                        float *p = I.psi_y + 3 * st + ((int64_t)ys * nz + z) * nx + x;
+                        float *p = H.psy + 3 * st + ((int64_t)ys * nz + z) * nx + x;
                         const float a = cy_a, b = cy_b;
                         q4 = b * p9[3] + a * dtyy_dy;
                         q5 = b * p9[4] + a * dtxy_dy;
@@ -519,7 +548,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     if (z >= nz - W) {
                         const int zs = z - (nz - W);
                         const int64_t st = (int64_t)ny * W * nx;
-                        float *p = I.psi_z + 3 * st + ((int64_t)y * W + zs) * nx + x;
+                        float *p = H.psz + 3 * st + ((int64_t)y * W + zs) * nx + x;
                         const float a = cz_a[h], b = cz_b[h];
                         q7 = b * p9[6] + a * dtzz_dz;
                         q8 = b * p9[7] + a * dtxz_dz;
@@ -534,7 +563,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
                     const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
                     const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
-                    const float k = I.k;
+                    const float k = H.k;
                     nvx = nvx + k * b_x * ((dtxx_dx + q1) + (dtxy_dy + q5) + (dtxz_dz + q8));
                     nvy = nvy + k * b_y * ((dtxy_dx + q2) + (dtyy_dy + q4) + (dtyz_dz + q9));
                     nvz = nvz + k * b_z * ((dtxz_dx + q3) + (dtyz_dy + q6) + (dtzz_dz + q7));
@@ -549,9 +578,9 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                         nvz = __fadd_rn(nvz, I.res[2 * ntr + o]);
                     }
                 }
-                I.f.v[0][c] = nvx;
-                I.f.v[1][c] = nvy;
-                I.f.v[2][c] = nvz;
+                H.out[c] = nvx;
+                H.out[H.nc + c] = nvy;
+                H.out[2 * H.nc + c] = nvz;
                 if (PASS == EFM_FWD) {
                     if (rec && I.gather != nullptr) {
                         const int64_t ntr = (int64_t)I.nt * I.nrec;
@@ -562,14 +591,14 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                             I.gather[2 * ntr + o] = nvz;
                         }
                     }
-                    if (I.border != nullptr) {
+                    if (border != nullptr) {
                         int64_t slot[3];
                         const int nslot = efm_strip_slots(I, x, y, z, slot);
-                        float *s = I.border + (int64_t)it * 3 * I.strip_n;
+                        float *s = border + (int64_t)it * 3 * strip_n;
                         for (int q = 0; q < nslot; ++q) {
                             s[slot[q]] = nvx;
-                            s[I.strip_n + slot[q]] = nvy;
-                            s[2 * I.strip_n + slot[q]] = nvz;
+                            s[strip_n + slot[q]] = nvy;
+                            s[2 * strip_n + slot[q]] = nvz;
                         }
                     }
                 }

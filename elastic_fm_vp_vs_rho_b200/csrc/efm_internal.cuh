@@ -102,10 +102,9 @@ __device__ __forceinline__ void efm_cell(const EfmInst &I, int block, int &x, in
 // Storage per component and step: X faces [4][by][bz], Y faces [4][bz][bx], Z faces
 // [4][by][bx] with bx = nx-2W, by = ny-2W, bz = nz-W-2.  Returns how many slots (0..3)
 // this cell owns and writes their offsets into slot[].
-__device__ __forceinline__ int efm_strip_slots(const EfmInst &I, int x, int y, int z,
-                                               int64_t slot[3]) {
-    const int W = I.W;
-    const int bx = I.nx - 2 * W, by = I.ny - 2 * W, bz = I.nz - W - 2;
+__device__ __forceinline__ int efm_strip_slots_v(int nx, int ny, int nz, int W, int x, int y,
+                                                 int z, int64_t slot[3]) {
+    const int bx = nx - 2 * W, by = ny - 2 * W, bz = nz - W - 2;
     const int xr = x - W, yr = y - W, zr = z - 2;
     if (xr < 0 || xr >= bx || yr < 0 || yr >= by || zr < 0 || zr >= bz) return 0;
     int n = 0;
@@ -118,6 +117,11 @@ __device__ __forceinline__ int efm_strip_slots(const EfmInst &I, int x, int y, i
     int pl = zr < 2 ? zr : (zr >= bz - 2 ? 2 + (zr - (bz - 2)) : -1);
     if (pl >= 0) slot[n++] = offZ + ((int64_t)pl * by + yr) * bx + xr;
     return n;
+}
+
+__device__ __forceinline__ int efm_strip_slots(const EfmInst &I, int x, int y, int z,
+                                               int64_t slot[3]) {
+    return efm_strip_slots_v(I.nx, I.ny, I.nz, I.W, x, y, z, slot);
 }
 
 // First index j with rec_lin[j] == c, or -1.

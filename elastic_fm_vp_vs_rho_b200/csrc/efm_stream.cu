@@ -142,6 +142,7 @@ struct Hot {
     float *psx, *psy, *psz;
     int64_t nc;       // cells per volume
     float k;
+    int nx, ny, nz, W;
 };
 
 __device__ __forceinline__ Hot make_hot(const EfmInst &I, float *out) {
@@ -152,6 +153,10 @@ __device__ __forceinline__ Hot make_hot(const EfmInst &I, float *out) {
     h.psz = I.psi_z;
     h.nc = (int64_t)I.nx * I.ny * I.nz;
     h.k = I.k;
+    h.nx = I.nx;
+    h.ny = I.ny;
+    h.nz = I.nz;
+    h.W = I.W;
     return h;
 }
 
@@ -160,7 +165,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
                                             int sp, int it, int x, int y, int z, int hidx,
                                             int cidx, bool has_src, const float *pp, const Coef &C,
                                             const Hot &H) {
-    const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+    const int nx = H.nx, ny = H.ny, nz = H.nz, W = H.W;
     const float *vx0 = R.halo(s0, 0), *vy0 = R.halo(s0, 1), *vz0 = R.halo(s0, 2);
     const float *rm0 = R.halo(s0, 3), *rm1 = R.halo(sp, 3);
     const float vxc = vx0[hidx], vyc = vy0[hidx], vzc = vz0[hidx];
@@ -276,7 +281,7 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
 template <int FIRST>
 __device__ __forceinline__ void load_psi(const EfmInst &I, const Hot &H, int x, int y, int z,
                                          float *pp) {
-    const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+    const int nx = H.nx, ny = H.ny, nz = H.nz, W = H.W;
 #pragma unroll
     for (int q = 0; q < 9; ++q) pp[q] = 0.f;
     if (x < W || x >= nx - W) {
@@ -459,7 +464,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                 float nvx = 0.f, nvy = 0.f, nvz = 0.f;
                 const bool zone = x < W || x >= nx - W || y < W || y >= ny - W || z >= nz - W;
                 int64_t slot[3];
-                const int nslot = zone ? 0 : efm_strip_slots(I, x, y, z, slot);
+                const int nslot = zone ? 0 : efm_strip_slots_v(nx, ny, nz, W, x, y, z, slot);
                 if (nslot > 0) {
                     const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
                     nvx = sv[slot[0]];
@@ -593,7 +598,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     }
                     if (border != nullptr) {
                         int64_t slot[3];
-                        const int nslot = efm_strip_slots(I, x, y, z, slot);
+                        const int nslot = efm_strip_slots_v(nx, ny, nz, W, x, y, z, slot);
                         float *s = border + (int64_t)it * 3 * strip_n;
                         for (int q = 0; q < nslot; ++q) {
                             s[slot[q]] = nvx;

@@ -605,7 +605,7 @@ class Elastic3D:
         mk.d_Rho.copy_(rho)
 
     def fwi_Vp_Vs_Rho(self, data_obs, listaTM, nIter, flagSave=False, tolFWI=1e-5,
-                      lbfgsLayers=10, ite_cte=2):
+                      lbfgsLayers=10, ite_cte=2, checkpoint=None, resume=False, log_path=None):
         """Multi-earthquake lambda/mu inversion (:2349-2719).
 
         Per iteration: forward + misfit + reverse-time gradient of every earthquake (one
@@ -613,7 +613,16 @@ class Elastic3D:
         update; then either a fixed-length step (iterations < ite_cte) or an L-BFGS step with
         backtracking (alpha = 1/2, 1/4, ..., 10 trials; NaN or the 10th trial reverts).
         rho follows Vp through the polynomial of compute_Rho; the top 10 planes of rho
-        are kept."""
+        are kept.
+
+        checkpoint: .npz path written after every iteration with the model, the three
+        L-BFGS histories, the cost history and the iteration -- the reference saves models per
+        iteration and resumes by hand (:2711-2719, the commented "Cargar" blocks :3095-3100);
+        resume=True continues from that file (the continued run equals an uninterrupted one
+        bit for bit).  log_path: one JSON line per iteration (misfit, step kind, alpha,
+        line-search trials, seconds)."""
+        import json
+        import time
         torch = _torch()
         self.costFunction = []
         mk = self.mk
@@ -621,6 +630,22 @@ class Elastic3D:
         L = int(lbfgsLayers)
         skL = torch.zeros((L,) + shape, dtype=torch.float32, device="cuda")
         ykL, skM, ykM, skR, ykR = (torch.zeros_like(skL) for _ in range(5))
+        hist = (skL, ykL, skM, ykM, skR, ykR)
+        hist_names = ("skL", "ykL", "skM", "ykM", "skR", "ykR")
+        start = 0
+        if resume and checkpoint and os.path.exists(checkpoint):
+            with np.load(checkpoint) as ck:
+                if int(ck["lbfgs_layers"]) != L or tuple(ck["Lambda"].shape) != shape:
+                    raise ValueError("checkpoint does not match this inversion")
+                start = int(ck["iteration"]) + 1
+                self.costFunction = [float(v) for v in ck["costFunction"]]
+                for name in ("Lambda", "Mu", "Rho"):
+                    setattr(mk, name, ck[name].astype(np.float32))
+                    getattr(mk, "d_" + name).copy_(torch.as_tensor(ck[name]).cuda())
+                mk.compute_Vp_Vs()
+                for t, name in zip(hist, hist_names):
+                    t.copy_(torch.as_tensor(ck[name]).cuda())
+        logf = open(log_path, "a") if log_path else None
         eng = self._all_shots_engine(listaTM)
         lo, hi = self._shard
         obs_flat = torch.cat([torch.as_tensor(np.stack([d.Vx, d.Vy, d.Vz]).astype(np.float32))
@@ -629,7 +654,9 @@ class Elastic3D:
         tmp = torch.empty(shape, dtype=torch.float32, device="cuda")
         nTry = 10
         self.fwi_gradients = None
-        for it in range(nIter):
+        for it in range(start, nIter):
+            t_it = time.time()
+            step_kind, alpha_used, trials = "fixed", None, 0
             total, g = self._shots_misfit(eng, obs_flat, True)
             gL, gM, gR = g[0].contiguous(), g[1].contiguous(), g[2].contiguous()
             for v in (gR, gM, gL):
@@ -675,6 +702,8 @@ class Elastic3D:
                     mk.d_Mu.copy_(cM - alpha * rM)
                     self._update_vp_vs_rho(cR_top)
                     self.costFunction[it] = optimal
+                step_kind = "lbfgs" if accepted else "reverted"
+                alpha_used, trials = alpha, tries
             else:
                 # fixed step with per-parameter scales (:2666-2702)
                 aL = 1e-5 * math.sqrt(_sumsq(mk.d_Lambda)) / float(gL.max().item())
@@ -687,6 +716,20 @@ class Elastic3D:
             mk.deviceToHost()
             if self.results_dir:
                 self._save_fwi(gL, gM, gR)
+            if checkpoint and _dist.world()[0] == 0:
+                tmp_path = checkpoint + ".tmp.npz"
+                np.savez(tmp_path, iteration=it, lbfgs_layers=L,
+                         costFunction=np.array(self.costFunction, np.float64),
+                         Lambda=mk.Lambda, Mu=mk.Mu, Rho=mk.Rho,
+                         **{n: t.cpu().numpy() for t, n in zip(hist, hist_names)})
+                os.replace(tmp_path, checkpoint)
+            if logf:
+                logf.write(json.dumps({"iteration": it, "misfit": self.costFunction[it],
+                                       "step": step_kind, "alpha": alpha_used,
+                                       "trials": trials, "seconds": time.time() - t_it}) + "\n")
+                logf.flush()
+        if logf:
+            logf.close()
         eng.close()
         return self.costFunction
 

@@ -11,7 +11,10 @@ references to the tensors it was given so their memory outlives the calls that u
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
+import math
+import warnings
 from dataclasses import dataclass
 
 import numpy as np
@@ -19,6 +22,26 @@ import numpy as np
 from . import _lib
 from ._lib import (EFM_GRAD_EXACT, EFM_GRAD_MODEL, EFM_GRAD_MT, EFM_GRAD_NT1, EFM_MAX_SRC,
                    EFM_SAVE_CHECKPOINTS, EFM_SAVE_STRIPS, check, ptr, stream_ptr)
+
+
+CFL_LIMIT = 1.0 / math.sqrt(3.0)  # Vp dt / dx bound of the 3-D second-order staggered scheme
+
+
+@contextlib.contextmanager
+def _range(name):
+    """NVTX range (visible to Nsight tools; no cost without them)."""
+    import torch
+    torch.cuda.nvtx.range_push(name)
+    try:
+        yield
+    finally:
+        torch.cuda.nvtx.range_pop()
+
+
+def courant_number(lam, mu, rho, dt, dx):
+    """max Vp * dt / dx of a model given as lambda, mu, rho tensors (Vp^2 = (lambda+2mu)/rho)."""
+    vp2 = ((lam + 2.0 * mu) / rho).max()
+    return math.sqrt(max(float(vp2), 0.0)) * dt / dx
 
 
 def _f32(t):
@@ -113,6 +136,10 @@ class ShotBatch:
                 raise ValueError(f"model arrays must have shape (ny, nz, nx)=({ny}, {nz}, {nx})")
         if wav.numel() < nt:
             raise ValueError("wavelet shorter than nt")
+        c = courant_number(lam, mu, rho, float(dt), float(dx))
+        if not c <= CFL_LIMIT:
+            warnings.warn(f"Courant number Vp*dt/dx = {c:.3f} exceeds {CFL_LIMIT:.3f}: the "
+                          "explicit scheme is unstable for this model / time step", RuntimeWarning)
         d = _lib.InstanceDesc(nx=nx, ny=ny, nz=nz, lenpml=lenpml, dx=float(dx), dt=float(dt),
                               nt=nt, cpml_host=cp.ctypes.data, lam_dev=lam.data_ptr(),
                               mu_dev=mu.data_ptr(), rho_dev=rho.data_ptr(),
@@ -180,7 +207,8 @@ class ShotBatch:
         if out is None:
             out = torch.empty(self.gather_size, dtype=torch.float32, device="cuda")
         save = (EFM_SAVE_STRIPS if save_borders else 0) | (EFM_SAVE_CHECKPOINTS if checkpoints else 0)
-        check(self._L.efm_forward(self._ctx, ptr(out), save, stream_ptr(stream)))
+        with _range("efm_forward"):
+            check(self._L.efm_forward(self._ctx, ptr(out), save, stream_ptr(stream)))
         return out
 
     def residual_misfit(self, mod, obs, res=None, stream=None):
@@ -232,10 +260,11 @@ class ShotBatch:
                             device="cuda")
         if mt:
             m = torch.empty((len(self.infos), EFM_MAX_SRC, 6), dtype=torch.float64, device="cuda")
-        check(self._L.efm_gradient(self._ctx, ptr(res.contiguous()),
-                                   ptr(g) if g is not None else None,
-                                   ptr(m) if m is not None else None, flags,
-                                   stream_ptr(stream)))
+        with _range("efm_gradient"):
+            check(self._L.efm_gradient(self._ctx, ptr(res.contiguous()),
+                                       ptr(g) if g is not None else None,
+                                       ptr(m) if m is not None else None, flags,
+                                       stream_ptr(stream)))
         return g, m
 
 

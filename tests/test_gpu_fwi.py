@@ -117,3 +117,35 @@ def test_cross_correlation_through_elastic3d(golden_refscale, cuda, tmp_path):
         assert (tmp_path / f"Gathers/modData0.{comp}.npy").exists()
         assert (tmp_path / f"Gathers/resData0.{comp}.npy").exists()
     assert (tmp_path / "TM/Mmodxx0.npy").exists() and (tmp_path / "CostFunction/costFunction0.npy").exists()
+
+
+def test_fwi_checkpoint_resume_equals_uninterrupted(golden_refscale, cuda, tmp_path):
+    """Two iterations + resume to three = three iterations in one go (bit for bit); the
+    JSONL log has one line per iteration."""
+    import json
+    from elastic_fm_vp_vs_rho_b200 import Elastic3D, Gather, StressTensor
+    d = golden_refscale
+
+    def run(n, ck=None, resume=False, log=None):
+        mt, m0, w, cp, geo = _setup(d)
+        e = Elastic3D(m0, geo, w, cp, mode=1)
+        e.setModel(m0)
+        obs = []
+        for k in range(len(d["src"])):
+            g = Gather(int(d["nt"]), len(d["rec_x"]))
+            g.Vx, g.Vy, g.Vz = d[f"obs{k}"]
+            obs.append(g)
+        cost = e.fwi_Vp_Vs_Rho(obs, [StressTensor(*d["mt_obs"])] * len(obs), n, lbfgsLayers=4,
+                               ite_cte=1, checkpoint=ck, resume=resume, log_path=log)
+        return list(cost), e.mk.Lambda.copy(), e.mk.Mu.copy(), e.mk.Rho.copy()
+
+    full = run(3)
+    ck, log = str(tmp_path / "fwi.npz"), str(tmp_path / "fwi.jsonl")
+    run(2, ck=ck, log=log)
+    part = run(3, ck=ck, resume=True, log=log)
+    assert part[0] == full[0]
+    for a, b in zip(part[1:], full[1:]):
+        assert np.array_equal(a, b)
+    lines = [json.loads(x) for x in open(log)]
+    assert [x["iteration"] for x in lines] == [0, 1, 2]
+    assert lines[2]["step"] in ("lbfgs", "reverted") and lines[0]["step"] == "fixed"

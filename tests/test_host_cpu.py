@@ -79,3 +79,17 @@ def test_oracle_border_and_zone_masks_are_disjoint_where_it_matters():
     box = ~z
     assert (b & box).sum() > 0
     assert np.all(~z[:, 2:4, W:nx - W][W:ny - W])
+
+
+def test_courant_number_and_warning():
+    """CPU: the stability check ShotBatch.add applies (Vp dt / dx against 1/sqrt(3))."""
+    import math
+
+    import torch
+    from elastic_fm_vp_vs_rho_b200.engine import CFL_LIMIT, courant_number
+    rho = torch.full((2, 2, 2), 2000.0)
+    mu = rho * 1500.0 ** 2
+    lam = rho * 3000.0 ** 2 - 2 * mu
+    c = courant_number(lam, mu, rho, 1e-3, 10.0)
+    assert abs(c - 0.3) < 1e-6
+    assert CFL_LIMIT == 1.0 / math.sqrt(3.0)

@@ -54,7 +54,8 @@ constexpr int CV_ASLAB = CV_AROWS * 16;    // bytes of one 8-channel slab
 constexpr int CV_STAGES = 4;               // weight-gradient ring depth
 constexpr int CV_MAX_STAGES = 8;
 constexpr int CV_SMEM_BUDGET = 200 * 1024; // forward ring: as deep as fits next to the weights
-constexpr int CV_R = 4;                    // output z rows per forward tile
+// output z rows per forward tile: double-buffered accumulators of R x cout TMEM columns
+__host__ __device__ constexpr int cv_rows(int cout) { return 256 / cout > 8 ? 8 : 256 / cout; }
 constexpr int CV_THREADS = 192;            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int CV_MIN_SMEM = 116 * 1024;    // one block per SM: TMEM allocation never waits
 constexpr int WG_K = 128;                  // voxels per weight-gradient K chunk
@@ -146,9 +147,11 @@ __device__ __forceinline__ void store_bf16x8(__nv_bfloat16 *dst, const float *v)
 
 // ------------------------------------------------------------------ forward / data gradient
 // MODE 0: y = act(conv(x) + bias) (bf16 and/or fp32 out); MODE 1: y = conv(x) * [mask > 0].
-// A tile is CV_MT voxels along x times CV_R consecutive z rows (one accumulator each); the
-// 3 (CV_R + 2) input rows (kd, zi) it reads arrive one slab per stage and feed every output
-// row r with kh = zi - r in 0..2.
+// A tile is CV_MT voxels along x times R consecutive z rows (one accumulator each); the
+// 3 (R + 2) input rows (kd, zi) it reads arrive one slab per stage.  One MMA per (slab, kw,
+// 16 input channels) covers every output row in reach at once: its N dimension stacks the
+// kh taps (rows kh x cout of the weight slab (kd, kw)) and writes the accumulators of rows
+// zi - kh, which TMEM keeps in descending row order so that they are adjacent columns.
 template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(CV_THREADS, 1)
 efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_w,
@@ -158,11 +161,14 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 64 && CIN <= 64, "channels");
     constexpr int NG = CIN / 8;                       // 8-channel groups (K core matrices)
     constexpr int WBYTES = 27 * CIN * COUT * 2;
+    constexpr int WSLAB = 3 * COUT * 16;              // weight slab (g, kd, kw): rows kh x cout
     constexpr int ASTAGE = NG * CV_ASLAB;
-    constexpr int R = CV_R;
+    constexpr int R = cv_rows(COUT);
     constexpr int NSLAB = 3 * (R + 2);                // input rows per tile
     constexpr int NST = cv_fwd_stages(WBYTES, ASTAGE);
-    constexpr uint32_t IDESC = efm_idesc_bf16(CV_MT, COUT, false, false);
+    constexpr uint32_t ID1 = efm_idesc_bf16(CV_MT, COUT, false, false);
+    constexpr uint32_t ID2 = efm_idesc_bf16(CV_MT, 2 * COUT, false, false);
+    constexpr uint32_t ID3 = efm_idesc_bf16(CV_MT, 3 * COUT, false, false);
     constexpr uint32_t NCOLS = 2 * R * COUT <= 32 ? 32 : 2 * R * COUT;  // double-buffered
     static_assert(2 * R * COUT <= 512, "TMEM columns");
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -181,8 +187,12 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
         efm_prefetch_tmap(&tm_x);
         efm_prefetch_tmap(&tm_w);
         efm_mbar_expect_tx(&S.wbar, WBYTES);
+        // weight slab (g, kd, kw) <- taps (kd, 0..2, kw) of channel group g: rows [kh][cout]
         for (int g = 0; g < NG; ++g)
-            efm_tma_load_3d(wsm + g * 27 * COUT * 16, &tm_w, &S.wbar, 8 * g, 0, 0);
+            for (int kd = 0; kd < 3; ++kd)
+                for (int kw = 0; kw < 3; ++kw)
+                    efm_tma_load_4d(wsm + ((g * 3 + kd) * 3 + kw) * WSLAB, &tm_w, &S.wbar, 8 * g, 0,
+                                    kw, 3 * kd);
         int st = 0;
         uint32_t ph = 0;
         uint32_t issued_parity[NST];
@@ -215,34 +225,40 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
         // ---------------- MMA issuer
         bool ok = cv_wait(&S.wbar, 0, abort);
         const uint32_t abase = efm_smem_addr(asm_);
-        const uint64_t wdesc = efm_sdesc(efm_smem_addr(wsm), 27 * COUT * 16, 128);
+        const uint64_t wdesc = efm_sdesc(efm_smem_addr(wsm), 9 * WSLAB, 128);
         int st = 0, acc = 0;
         uint32_t ph = 0, aph = 0;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
             if (!cv_wait(&S.tempty[acc], aph ^ 1u, abort)) { ok = false; break; }
             efm_tc_fence_after();
-            uint32_t started = 0;  // bit r: accumulator of output row r holds a partial sum
             for (int k = 0; k < NSLAB && ok; ++k) {
                 const int kd = k / (R + 2), zi = k % (R + 2);
                 if (!cv_wait(&S.full[st], ph, abort)) { ok = false; break; }
                 efm_tc_fence_after();
-                // descriptors differ only in their start-address field: build one per stage
-                // / tap row and add the (compile-time) offsets >> 4 for kw and j
+                // taps kh_lo..kh_hi reach output rows zi - kh inside the tile; the accumulator
+                // of row r sits at column block R-1-r, so row zi - kh_lo comes first
+                const int kh_lo = zi - R + 1 > 0 ? zi - R + 1 : 0, kh_hi = zi < 2 ? zi : 2;
+                const uint32_t dcol = S.tmem + (acc * R + (R - 1 - (zi - kh_lo))) * COUT;
                 const uint64_t adesc = efm_sdesc(abase + st * ASTAGE, CV_ASLAB, 128);
+                const uint64_t bk = wdesc + (uint64_t)((kd * 3 * WSLAB + kh_lo * COUT * 16) >> 4);
+                // a row's first contribution is (kd 0, kh 0, kw 0, j 0): that MMA may not
+                // accumulate, so it runs apart from the rows already started
+                const bool fresh = kd == 0 && kh_lo == 0;
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const int kh = zi - r;
-                    if (kh < 0 || kh > 2) continue;
-                    const uint32_t d = S.tmem + (acc * R + r) * COUT;
-                    const uint64_t bdesc = wdesc + (uint64_t)(((kd * 9 + kh * 3) * COUT * 16) >> 4);
+                for (int kw = 0; kw < 3; ++kw) {
 #pragma unroll
-                    for (int kw = 0; kw < 3; ++kw) {
-#pragma unroll
-                        for (int j = 0; j < CIN / 16; ++j) {
-                            const uint64_t a = adesc + (uint64_t)((2 * j * CV_ASLAB + (kw + 3) * 16) >> 4);
-                            const uint64_t b = bdesc + (uint64_t)(((2 * j * 27 + kw) * COUT * 16) >> 4);
-                            efm_mma_bf16(d, a, b, IDESC, (started >> r) & 1u);
-                            started |= 1u << r;
+                    for (int j = 0; j < CIN / 16; ++j) {
+                        const uint64_t a = adesc + (uint64_t)((2 * j * CV_ASLAB + (kw + 3) * 16) >> 4);
+                        const uint64_t b = bk + (uint64_t)((2 * j * 9 * WSLAB + kw * WSLAB) >> 4);
+                        const int n = kh_hi - kh_lo + 1;
+                        if (fresh && kw == 0 && j == 0) {
+                            efm_mma_bf16(dcol, a, b, ID1, 0u);
+                            if (n == 2)
+                                efm_mma_bf16(dcol + COUT, a, b + ((COUT * 16) >> 4), ID1, 1u);
+                            else if (n == 3)
+                                efm_mma_bf16(dcol + COUT, a, b + ((COUT * 16) >> 4), ID2, 1u);
+                        } else {
+                            efm_mma_bf16(dcol, a, b, n == 1 ? ID1 : n == 2 ? ID2 : ID3, 1u);
                         }
                     }
                 }
@@ -260,6 +276,9 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
         const int row = q * 32 + lane;    // voxel of the tile
         int acc = 0;
         uint32_t aph = 0;
+        float bv[COUT];
+#pragma unroll
+        for (int c = 0; c < COUT; ++c) bv[c] = (MODE == 0 && bias) ? bias[c] : 0.f;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             if (!cv_wait(&S.tfull[acc], aph, abort)) break;
             efm_tc_fence_after();
@@ -267,16 +286,23 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
             const int x = x0 + row;
             for (int r = 0; r < R; ++r) {
                 float v[COUT];
+                {
+                    uint32_t raw[COUT];
 #pragma unroll
-                for (int c = 0; c < COUT; c += 16)
-                    efm_tmem_ld16(S.tmem + ((uint32_t)(q * 32) << 16) + (acc * R + r) * COUT + c, v + c);
+                    for (int c = 0; c < COUT; c += 16)
+                        efm_tmem_ld16_nowait(S.tmem + ((uint32_t)(q * 32) << 16) + (acc * R + (R - 1 - r)) * COUT + c,
+                                             raw + c);
+                    efm_tmem_wait_ld();  // one wait for the row's COUT / 16 loads
+#pragma unroll
+                    for (int c = 0; c < COUT; ++c) v[c] = __uint_as_float(raw[c]);
+                }
                 const int z = z0 + r;
                 if (x >= nx || z >= nz) continue;
                 const int64_t vox = ((int64_t)y * nz + z) * nx + x;
                 if (MODE == 0) {
 #pragma unroll
                     for (int c = 0; c < COUT; ++c) {
-                        float u = v[c] + (bias ? bias[c] : 0.f);
+                        float u = v[c] + bv[c];
                         v[c] = (relu && u < 0.f) ? 0.f : u;
                     }
                     if (y_f32) {
@@ -406,9 +432,13 @@ efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_con
             for (int kw = 0; kw < 3; ++kw) {
                 float v[COUT];
                 if (have) {
+                    uint32_t raw[COUT];
 #pragma unroll
                     for (int c = 0; c < COUT; c += 16)
-                        efm_tmem_ld16(S.tmem + ((uint32_t)(qd * 32) << 16) + kw * COUT + c, v + c);
+                        efm_tmem_ld16_nowait(S.tmem + ((uint32_t)(qd * 32) << 16) + kw * COUT + c, raw + c);
+                    efm_tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < COUT; ++c) v[c] = __uint_as_float(raw[c]);
                 } else {
 #pragma unroll
                     for (int c = 0; c < COUT; ++c) v[c] = 0.f;
@@ -528,15 +558,17 @@ int map_volume(CUtensorMap *m, const void *base, const efm_conv_desc *d, int c, 
     return EFM_OK;
 }
 
-// weights [27][cout][cin] BF16; box (8, cout, 27)
+// weights [27][cout][cin] BF16 seen as (cin, cout, kw, 3 kd + kh); box (8, cout, 1, 3): the
+// three kh taps of one (kd, kw) as consecutive rows
 int map_weights(CUtensorMap *m, const void *base, int cin, int cout) {
     auto enc = conv_encoder();
     if (!enc) return efm_internal_fail(EFM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    cuuint64_t dims[3] = {(cuuint64_t)cin, (cuuint64_t)cout, 27};
-    cuuint64_t strides[2] = {(cuuint64_t)cin * 2, (cuuint64_t)cin * cout * 2};
-    cuuint32_t box[3] = {8, (cuuint32_t)cout, 27};
-    cuuint32_t es[3] = {1, 1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides,
+    cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)cout, 3, 9};
+    cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)cin * cout * 2,
+                             (cuuint64_t)3 * cin * cout * 2};
+    cuuint32_t box[4] = {8, (cuuint32_t)cout, 1, 3};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides,
                      box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
@@ -576,7 +608,8 @@ int launch_fwd(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap 
     auto k = efm_conv_fwd_kernel<CIN, COUT, MODE>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
-    const int64_t tiles = (int64_t)((d->nx + CV_MT - 1) / CV_MT) * ((d->nz + CV_R - 1) / CV_R) * d->ny;
+    constexpr int R = cv_rows(COUT);
+    const int64_t tiles = (int64_t)((d->nx + CV_MT - 1) / CV_MT) * ((d->nz + R - 1) / R) * d->ny;
     const int grid = (int)(tiles < num_sms() ? tiles : num_sms());
     k<<<grid, CV_THREADS, smem, s>>>(tx, tw, d->nx, d->ny, d->nz, bias, relu,
                                       static_cast<const __nv_bfloat16 *>(mask),

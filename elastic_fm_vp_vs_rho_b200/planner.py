@@ -64,7 +64,9 @@ def choose_checkpoint_interval(nx, ny, nz, lenpml, nt, budget, nrec=0):
 def plan(sizes, budget):
     """sizes: bytes per instance.  Returns sub-batches (lists of indices, each sub-batch in
     ascending index order) whose totals are <= budget; raises if one instance alone does
-    not fit."""
+    not fit.  First fit (largest first) fixes the number of sub-batches; the instances are
+    then spread over that many sub-batches as evenly as the budget allows (largest first
+    into the least-loaded), so no sub-batch is left with a small tail of work."""
     order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
     bins, loads = [], []
     for i in order:
@@ -78,7 +80,15 @@ def plan(sizes, budget):
         else:
             bins.append([i])
             loads.append(sizes[i])
-    return [sorted(b) for b in bins]
+    k = len(bins)
+    even, eload = [[] for _ in range(k)], [0] * k
+    for i in order:
+        b = min(range(k), key=lambda j: eload[j])
+        if eload[b] + sizes[i] > budget:
+            return [sorted(x) for x in bins]  # balancing does not fit: keep first fit
+        even[b].append(i)
+        eload[b] += sizes[i]
+    return [sorted(x) for x in even]
 
 
 def device_budget(fraction=0.85, reserve=2 << 30):

@@ -20,6 +20,8 @@ def test_instance_bytes_orders_and_plan_fits():
     assert len(bins) <= 5
     with pytest.raises(MemoryError):
         planner.plan([11], 10)
+    # 32 equal shots, 30 fit: two sub-batches of 16, not 30 + 2
+    assert sorted(len(b) for b in planner.plan([6] * 32, 180)) == [16, 16]
 
 
 def test_checkpoint_interval_minimises_exact_workspace():

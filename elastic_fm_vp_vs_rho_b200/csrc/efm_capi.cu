@@ -26,6 +26,7 @@ extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, int ring,
                                          const EfmInst *insts, int ninst, int tiles, int it,
                                          cudaStream_t s);
 extern "C" cudaError_t efm_stream_init_attributes();
+extern "C" void efm_stream_set_pdl(int enable);
 extern "C" cudaError_t efm_launch_pair(int which, int rows, int ring, const EfmInst *ts,
                                        int tiles_s, const EfmInst *tv, int tiles_v, int ninst,
                                        int it, cudaStream_t s);
@@ -149,6 +150,7 @@ struct efm_ctx {
     int opt_rows = 0;
     int opt_ring = 0;
     int opt_pair = 1;
+    int opt_pdl = 1;
     int rows = 2;  // cells per thread of the tables last built for the streaming kernels
     int ring = 4;  // ring depth of those tables' kernels
     int opt_ck_every = 50;
@@ -520,6 +522,7 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
     const int n = (int)ctx->inst.size();
     const bool st = stream_ok(ctx);
     if (st && (rc = get_encoder())) return rc;
+    efm_stream_set_pdl(ctx->opt_pdl);
     const int rows = ctx->rows = ctx->opt_rows == 1 ? 1 : 2;
     const int ring = ctx->ring = (rows == 1 && ctx->opt_ring == 6) ? 6 : 4;
     const int tz = efm_st_tz(rows), hz = efm_st_hz(rows);
@@ -972,6 +975,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     const int n = (int)ctx->inst.size();
     const bool st = stream_ok(ctx);
     if (st && (rc = get_encoder())) return rc;
+    efm_stream_set_pdl(ctx->opt_pdl);
     const int rows = ctx->rows = ctx->opt_rows == 1 ? 1 : 2;
     const int ring = ctx->ring = (rows == 1 && ctx->opt_ring == 6) ? 6 : 4;
     const int tz = efm_st_tz(rows), hz = efm_st_hz(rows);
@@ -1184,6 +1188,7 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             ctx->opt_rows = value;
             break;
         case EFM_OPT_PAIR_LAUNCH: ctx->opt_pair = value != 0; break;
+        case EFM_OPT_PDL: ctx->opt_pdl = value != 0; break;
         case EFM_OPT_RING_DEPTH:
             if (value != 0 && value != 4 && value != 6) return fail(EFM_ERR_ARG, "ring depth must be 0, 4 or 6");
             ctx->opt_ring = value;

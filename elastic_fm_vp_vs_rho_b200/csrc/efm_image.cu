@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(IMG_THREADS, 3)
 efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ uint64_t hbar[IMG_RH], cbar[IMG_RC];
+    efm_pdl_trigger();
     const EfmInst &I = insts[efm_find_inst(insts, ninst, blockIdx.x)];
     if (it >= I.nsteps) return;
     const int lt = blockIdx.x - I.tile_begin;
@@ -103,6 +104,7 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         for (int s = 0; s < IMG_RC; ++s) efm_mbar_init(&cbar[s], 1);
         efm_fence_barrier_init();
     }
+    efm_pdl_wait();  // fields only after the preceding kernel has finished
     __syncthreads();
     const int hlast = ye;      // halo planes ys-2 .. ye (j+1 for j = ye-1)
     const int clast = ye - 1;  // cell planes ys .. ye-1
@@ -184,9 +186,18 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     }
 }
 
+extern "C" void efm_stream_pdl_config(cudaLaunchConfig_t *cfg, cudaLaunchAttribute *attr);
+
 extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int tiles, int it,
                                         cudaStream_t s) {
-    efm_image_stream<<<tiles, IMG_THREADS, IMG_SMEM, s>>>(insts, ninst, it);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(tiles);
+    cfg.blockDim = dim3(IMG_THREADS);
+    cfg.dynamicSmemBytes = IMG_SMEM;
+    cfg.stream = s;
+    efm_stream_pdl_config(&cfg, attr);
+    cudaLaunchKernelEx(&cfg, efm_image_stream, insts, ninst, it);
     return cudaGetLastError();
 }
 

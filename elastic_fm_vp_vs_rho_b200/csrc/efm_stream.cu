@@ -119,6 +119,9 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
         const unsigned lo = __ballot_sync(0xffffffffu, a), hi = __ballot_sync(0xffffffffu, b);
         if (l == 0) *s_recbits = (unsigned long long)lo | ((unsigned long long)hi << 32);
     }
+    // everything above reads only the call's static tables; the fields come after the
+    // preceding kernel has finished
+    efm_pdl_wait();
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int q = 0; q < NH + NC; ++q) efm_prefetch_tmap(tm + q);
@@ -320,6 +323,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     __shared__ uint64_t bars[SR];
     __shared__ int s_src;
     __shared__ unsigned long long s_rec;
+    efm_pdl_trigger();
     const EfmInst &I = insts[efm_find_inst(insts, ninst, block)];
     if (it >= I.nsteps) return;
     const Tile T = stream_tile<ROWS>(I, block);
@@ -399,6 +403,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     __shared__ uint64_t bars[SR];
     __shared__ int s_src;
     __shared__ unsigned long long s_rec;
+    efm_pdl_trigger();
     const EfmInst &I = insts[efm_find_inst(insts, ninst, block)];
     if (it >= I.nsteps) return;
     const Tile T = stream_tile<ROWS>(I, block);
@@ -667,21 +672,51 @@ constexpr int kSmemStress = efm_stream_smem(ROWS, SR, 4, 7);
 template <int ROWS, int SR>
 constexpr int kSmemVelocity = efm_stream_smem(ROWS, SR, 6, 4);
 
+// Launch with the programmatic-serialization attribute when enabled: the kernel's prologue
+// overlaps the tail of the preceding kernel (every streaming kernel waits in
+// efm_pdl_wait before it reads or writes fields).
+static int g_pdl = 1;
+
+extern "C" void efm_stream_set_pdl(int enable) { g_pdl = enable != 0; }
+
+// the programmatic-serialization attribute (when enabled) for another launcher's config
+extern "C" void efm_stream_pdl_config(cudaLaunchConfig_t *cfg, cudaLaunchAttribute *attr) {
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg->attrs = attr;
+    cfg->numAttrs = g_pdl ? 1 : 0;
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*k)(KArgs...), int grid, int smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(EFM_STHREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <int ROWS, int SR>
 static void launch_rows(int pass, int kind, const EfmInst *insts, int ninst, int tiles, int it,
                         cudaStream_t s) {
     constexpr int SS = kSmemStress<ROWS, SR>, SV = kSmemVelocity<ROWS, SR>;
     if (kind == 0) {
         switch (pass) {
-            case EFM_FWD: efm_stress_stream<EFM_FWD, ROWS, SR><<<tiles, EFM_STHREADS, SS, s>>>(insts, ninst, it); break;
-            case EFM_ADJ: efm_stress_stream<EFM_ADJ, ROWS, SR><<<tiles, EFM_STHREADS, SS, s>>>(insts, ninst, it); break;
-            default: efm_stress_stream<EFM_REV, ROWS, SR><<<tiles, EFM_STHREADS, SS, s>>>(insts, ninst, it); break;
+            case EFM_FWD: launch_k(efm_stress_stream<EFM_FWD, ROWS, SR>, tiles, SS, s, insts, ninst, it); break;
+            case EFM_ADJ: launch_k(efm_stress_stream<EFM_ADJ, ROWS, SR>, tiles, SS, s, insts, ninst, it); break;
+            default: launch_k(efm_stress_stream<EFM_REV, ROWS, SR>, tiles, SS, s, insts, ninst, it); break;
         }
     } else {
         switch (pass) {
-            case EFM_FWD: efm_velocity_stream<EFM_FWD, ROWS, SR><<<tiles, EFM_STHREADS, SV, s>>>(insts, ninst, it); break;
-            case EFM_ADJ: efm_velocity_stream<EFM_ADJ, ROWS, SR><<<tiles, EFM_STHREADS, SV, s>>>(insts, ninst, it); break;
-            default: efm_velocity_stream<EFM_REV, ROWS, SR><<<tiles, EFM_STHREADS, SV, s>>>(insts, ninst, it); break;
+            case EFM_FWD: launch_k(efm_velocity_stream<EFM_FWD, ROWS, SR>, tiles, SV, s, insts, ninst, it); break;
+            case EFM_ADJ: launch_k(efm_velocity_stream<EFM_ADJ, ROWS, SR>, tiles, SV, s, insts, ninst, it); break;
+            default: launch_k(efm_velocity_stream<EFM_REV, ROWS, SR>, tiles, SV, s, insts, ninst, it); break;
         }
     }
 }
@@ -692,9 +727,9 @@ static void launch_pair_rows(int which, const EfmInst *ts, int tiles_s, const Ef
     constexpr int SM = kSmemStress<ROWS, SR> > kSmemVelocity<ROWS, SR> ? kSmemStress<ROWS, SR>
                                                                        : kSmemVelocity<ROWS, SR>;
     if (which == 0)
-        efm_pair_stream<EFM_ADJ, EFM_REV, ROWS, SR><<<tiles_s + tiles_v, EFM_STHREADS, SM, s>>>(ts, tiles_s, tv, ninst, it);
+        launch_k(efm_pair_stream<EFM_ADJ, EFM_REV, ROWS, SR>, tiles_s + tiles_v, SM, s, ts, tiles_s, tv, ninst, it);
     else
-        efm_pair_stream<EFM_REV, EFM_ADJ, ROWS, SR><<<tiles_s + tiles_v, EFM_STHREADS, SM, s>>>(ts, tiles_s, tv, ninst, it);
+        launch_k(efm_pair_stream<EFM_REV, EFM_ADJ, ROWS, SR>, tiles_s + tiles_v, SM, s, ts, tiles_s, tv, ninst, it);
 }
 
 // which 0: adjoint stress (ts) + rebuild velocity (tv); 1: rebuild stress (ts) + adjoint

@@ -65,3 +65,15 @@ __device__ __forceinline__ void efm_tma_load_3d(void *dst, const CUtensorMap *m,
         "l"(m), "r"(efm_smem_addr(bar)), "r"(x), "r"(z), "r"(y)
         : "memory");
 }
+
+// Programmatic dependent launch: let the next kernel in the stream start its prologue now
+// (it still waits in efm_pdl_wait before touching anything this kernel writes) ...
+__device__ __forceinline__ void efm_pdl_trigger() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// ... and wait until the preceding kernel has completed and its writes are visible.  A no-op
+// when the kernel was launched without the programmatic-serialization attribute.
+__device__ __forceinline__ void efm_pdl_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}

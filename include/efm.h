@@ -198,6 +198,9 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 /* 1 (default): in the imaging gradient, launch the adjoint and rebuild half-steps of a
  * time step pairwise in one grid (they touch disjoint fields); 0: five launches per step. */
 #define EFM_OPT_PAIR_LAUNCH 6
+/* 1 (default): launch the plane-streaming kernels as programmatic dependents, so each one's
+ * prologue overlaps the tail of the previous kernel; 0: plain stream order. */
+#define EFM_OPT_PDL 7
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*

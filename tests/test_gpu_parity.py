@@ -321,8 +321,9 @@ def test_stream_kernels_match_thread_per_cell_kernels(golden_c1scale, cuda, ychu
 
 @pytest.mark.parametrize("rows,ring", [(2, 4), (1, 4), (1, 6)])
 def test_paired_gradient_launches_equal_sequential(golden_c1scale, cuda, rows, ring):
-    """The gradient's adjoint / rebuild half-steps launched pairwise in one grid give
-    bit-identical gradients to five launches per step."""
+    """The gradient's adjoint / rebuild half-steps launched pairwise in one grid, and with
+    programmatic dependent launches, give bit-identical gradients to five plain launches
+    per step."""
     from elastic_fm_vp_vs_rho_b200 import _lib
     d = golden_c1scale
     out = []
@@ -331,6 +332,7 @@ def test_paired_gradient_launches_equal_sequential(golden_c1scale, cuda, rows, r
         b.set_option(_lib.EFM_OPT_TILE_ROWS, rows)
         b.set_option(_lib.EFM_OPT_RING_DEPTH, ring)
         b.set_option(_lib.EFM_OPT_PAIR_LAUNCH, pair)
+        b.set_option(_lib.EFM_OPT_PDL, pair)
         mod = b.forward(save_borders=True)
         res, _ = b.residual_misfit(mod, cuda.as_tensor(d["obs0"].reshape(-1)).cuda())
         g, m = b.gradient(res, model=True, mt=True)

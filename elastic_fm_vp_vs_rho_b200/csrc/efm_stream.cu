@@ -674,8 +674,9 @@ constexpr int kSmemVelocity = efm_stream_smem(ROWS, SR, 6, 4);
 
 // Launch with the programmatic-serialization attribute when enabled: the kernel's prologue
 // overlaps the tail of the preceding kernel (every streaming kernel waits in
-// efm_pdl_wait before it reads or writes fields).
-static int g_pdl = 1;
+// efm_pdl_wait before it reads or writes fields).  Set by each efm_forward / efm_gradient
+// call from its context's option, per calling thread.
+static thread_local int g_pdl = 1;
 
 extern "C" void efm_stream_set_pdl(int enable) { g_pdl = enable != 0; }
 

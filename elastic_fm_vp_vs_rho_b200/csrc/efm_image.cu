@@ -197,8 +197,9 @@ extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int til
     cfg.dynamicSmemBytes = IMG_SMEM;
     cfg.stream = s;
     efm_stream_pdl_config(&cfg, attr);
-    cudaLaunchKernelEx(&cfg, efm_image_stream, insts, ninst, it);
-    return cudaGetLastError();
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, efm_image_stream, insts, ninst, it);
+    const cudaError_t l = cudaGetLastError();
+    return e != cudaSuccess ? e : l;
 }
 
 cudaError_t efm_image_init_attributes() {

@@ -688,6 +688,10 @@ extern "C" void efm_stream_pdl_config(cudaLaunchConfig_t *cfg, cudaLaunchAttribu
     cfg->numAttrs = g_pdl ? 1 : 0;
 }
 
+// Errors surface through the launcher's cudaGetLastError(); a failed cudaLaunchKernelEx is
+// recorded there too, but keep its own status for the first failure of a sequence.
+static thread_local cudaError_t g_launch_err = cudaSuccess;
+
 template <typename... KArgs, typename... Args>
 static void launch_k(void (*k)(KArgs...), int grid, int smem, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
@@ -700,7 +704,15 @@ static void launch_k(void (*k)(KArgs...), int grid, int smem, cudaStream_t s, Ar
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = g_pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, k, args...);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k, args...);
+    if (e != cudaSuccess && g_launch_err == cudaSuccess) g_launch_err = e;
+}
+
+static cudaError_t take_launch_err() {
+    const cudaError_t e = g_launch_err;
+    g_launch_err = cudaSuccess;
+    const cudaError_t l = cudaGetLastError();
+    return e != cudaSuccess ? e : l;
 }
 
 template <int ROWS, int SR>
@@ -744,7 +756,7 @@ extern "C" cudaError_t efm_launch_pair(int which, int rows, int ring, const EfmI
         launch_pair_rows<1, 4>(which, ts, tiles_s, tv, tiles_v, ninst, it, s);
     else
         launch_pair_rows<2, 4>(which, ts, tiles_s, tv, tiles_v, ninst, it, s);
-    return cudaGetLastError();
+    return take_launch_err();
 }
 
 // kind 0 = stress, 1 = velocity; rows = cells per thread (1 or 2) and ring = stages (4, or
@@ -758,7 +770,7 @@ extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, int ring,
         launch_rows<1, 4>(pass, kind, insts, ninst, tiles, it, s);
     else
         launch_rows<2, 4>(pass, kind, insts, ninst, tiles, it, s);
-    return cudaGetLastError();
+    return take_launch_err();
 }
 
 extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho, float *rmu,

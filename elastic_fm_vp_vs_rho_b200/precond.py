@@ -469,11 +469,17 @@ if __name__ == "__main__":
     ap.add_argument("--train", type=int, default=8, help="number of training seeds")
     ap.add_argument("--target", default="error", choices=["error", "update"])
     ap.add_argument("--test-seeds", default="7,8,9")
+    ap.add_argument("--grid", default="48,48,40", help="nx,ny,nz")
+    ap.add_argument("--nt", type=int, default=320)
+    ap.add_argument("--shots", type=int, default=4)
+    ap.add_argument("--receivers", type=int, default=8, help="per side of the surface grid")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
+    gx, gy, gz = (int(v) for v in a.grid.split(","))
+    spec = ProblemSpec(nx=gx, ny=gy, nz=gz, nt=a.nt, nshots=a.shots, nrec=a.receivers)
     r = experiment(train_seeds=tuple(range(100, 100 + a.train)),
                    test_seeds=tuple(int(v) for v in a.test_seeds.split(",")),
-                   iters=a.iters, epochs=a.epochs, target=a.target, log=print)
+                   iters=a.iters, epochs=a.epochs, spec=spec, target=a.target, log=print)
     s = json.dumps(r, indent=1)
     if a.out:
         with open(a.out, "w") as f:

@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--grid", default="128,128,96", help="nx,ny,nz")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-graph", action="store_true",
+                   help="launch the time loops step by step instead of replaying CUDA graphs")
     p.add_argument("--no-tune", action="store_true",
                    help="skip the launch-shape autotuner (default tile rows / y-chunk)")
     p.add_argument("--traffic-file", default=os.path.join(REPO, "profiles", "ncu_traffic.json"))
@@ -298,6 +300,7 @@ def main():
     if not args.no_tune:
         from elastic_fm_vp_vs_rho_b200 import autotune
         tuned = autotune.tune(eng, use_cache=False)
+    eng.set_option(_lib.EFM_OPT_GRAPH, 0 if args.no_graph else 1)
     L = _lib.load()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     red = torch.zeros(3 * w.ncells + 1, dtype=torch.float32, device="cuda")
@@ -406,7 +409,9 @@ def main():
                 "data": "synthetic (seeded layered + anomaly model, MT source)",
                 "config": dict(config_dict(w, args, world), launch_shape=tuned and {
                     "tile_rows": tuned["rows"], "ring": tuned.get("ring", 4), "ychunk": tuned["ychunk"],
-                    "source": "autotuned (probe of %d steps)" % tuned["nt_probe"]}),
+                    "source": "autotuned (probe of %d steps)" % tuned["nt_probe"]},
+                    time_loop="step launches" if args.no_graph else
+                    "CUDA graph per time loop (captured once, replayed)"),
                 "gpu_launches": gpu_launches,
                 "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
         print(json.dumps(line), flush=True)

@@ -32,6 +32,7 @@ EFM_OPT_TILE_ROWS = 4
 EFM_OPT_RING_DEPTH = 5
 EFM_OPT_PAIR_LAUNCH = 6
 EFM_OPT_PDL = 7
+EFM_OPT_GRAPH = 8
 EFM_NKERN = 11
 KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity",
                 "rev_stress", "residual_misfit", "model_reciprocals", "imaging",

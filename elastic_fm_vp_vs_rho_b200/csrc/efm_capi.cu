@@ -160,6 +160,14 @@ struct efm_ctx {
     int maps_cap = 0;
     unsigned int *d_err = nullptr;
     int tiles[16] = {};             // total tiles of each table slot (T_NSLOT <= 16)
+    // CUDA graphs of the time loops (0: forward, 1: gradient), replayed while the key holds
+    int opt_graph = 1;
+    cudaStream_t cap_stream = nullptr;  // private capture stream (the caller's may be legacy)
+    struct Loop {
+        std::vector<int64_t> key;
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches[EFM_NKERN] = {};
+    } loops[2];
 };
 
 // table slots of efm_ctx::d_tab (n entries each)
@@ -193,6 +201,60 @@ int timed_launch(efm_ctx *ctx, int kind, cudaStream_t s, F &&launch) {
         ctx->ev_used.push_back({kind, i0});
     }
     return EFM_OK;
+}
+
+// Run `body(stream)`, the launches of one time loop, either directly on `s` or through a CUDA
+// graph of it captured on a private stream the first time `key` is seen and replayed on `s`
+// afterwards.  The key holds everything the captured launches bake in: table addresses, grid
+// sizes, tile shape, options, step counts and the buffers of device-to-device copies.  The
+// tables themselves are uploaded before every call, so a replay reads the current call's
+// pointers and sizes.  Launch counters advance by the captured launches on every replay.
+template <class F>
+int run_loop(efm_ctx *ctx, int which, const std::vector<int64_t> &key, cudaStream_t s, F &&body) {
+    if (!ctx->opt_graph || ctx->timing) return body(s);
+    efm_ctx::Loop &L = ctx->loops[which];
+    if (L.exec == nullptr || L.key != key) {
+        if (L.exec != nullptr) {
+            EFM_CK(cudaGraphExecDestroy(L.exec));
+            L.exec = nullptr;
+        }
+        L.key.clear();
+        if (ctx->cap_stream == nullptr)
+            EFM_CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+        int64_t before[EFM_NKERN];
+        std::memcpy(before, ctx->launches, sizeof(before));
+        EFM_CK(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = body(ctx->cap_stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);
+        for (int k = 0; k < EFM_NKERN; ++k) {
+            L.launches[k] = ctx->launches[k] - before[k];
+            ctx->launches[k] = before[k];  // nothing ran yet
+        }
+        if (rc != EFM_OK || e != cudaSuccess) {
+            if (g != nullptr) cudaGraphDestroy(g);
+            if (rc != EFM_OK) return rc;
+            return fail(EFM_ERR_CUDA, std::string("time-loop capture: ") + cudaGetErrorString(e));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&L.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            L.exec = nullptr;
+            return fail(EFM_ERR_CUDA, std::string("time-loop graph: ") + cudaGetErrorString(ei));
+        }
+        L.key = key;
+    }
+    EFM_CK(cudaGraphLaunch(L.exec, s));
+    for (int k = 0; k < EFM_NKERN; ++k) ctx->launches[k] += L.launches[k];
+    return EFM_OK;
+}
+
+void drop_loops(efm_ctx *ctx) {
+    for (efm_ctx::Loop &L : ctx->loops) {
+        if (L.exec != nullptr) cudaGraphExecDestroy(L.exec);
+        L.exec = nullptr;
+        L.key.clear();
+    }
 }
 
 int collect_times(efm_ctx *ctx) {
@@ -731,6 +793,67 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
 }
 
 
+// One launch sequence of the imaging gradient's time loop (tables uploaded by efm_gradient).
+int gradient_loop(efm_ctx *ctx, bool st, bool model, int n, int maxsteps, cudaStream_t s) {
+    int rc;
+    auto dtab = [&](int k) { return (const EfmInst *)(ctx->d_tab + (size_t)k * n); };
+    for (int it = 0; it < maxsteps; ++it) {
+        if (st && model && ctx->opt_pair) {
+            // (adjoint stress | rebuild velocity), (rebuild stress | adjoint velocity), imaging:
+            // within a step the adjoint chain and the rebuild write disjoint fields, and the
+            // imaging reads neither the rebuild's stress nor anything the next step's first
+            // pair writes before this step's imaging has finished (stream order)
+            const int kv = (it & 1) ? T_REV_V1 : T_REV_V0, ks = (it & 1) ? T_REV_S1 : T_REV_S0;
+            const int ki = (it & 1) ? T_IMG1 : T_IMG0;
+            if ((rc = timed_launch(ctx, EFM_K_PAIR_ADJS_REVV, s, [&] {
+                     return efm_launch_pair(0, ctx->rows, ctx->ring, dtab(T_ADJ_S), ctx->tiles[T_ADJ_S],
+                                            dtab(kv), ctx->tiles[kv], n, it, s);
+                 })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_PAIR_REVS_ADJV, s, [&] {
+                     return efm_launch_pair(1, ctx->rows, ctx->ring, dtab(ks), ctx->tiles[ks],
+                                            dtab(T_ADJ_V), ctx->tiles[T_ADJ_V], n, it, s);
+                 })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_IMAGING, s, [&] {
+                     return efm_launch_image(dtab(ki), n, ctx->tiles[ki], it, s);
+                 })))
+                return rc;
+            continue;
+        }
+        if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
+                 return st ? efm_launch_stream(EFM_ADJ, 0, ctx->rows, ctx->ring, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
+                           : efm_launch_stress(EFM_ADJ, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s);
+             })))
+            return rc;
+        if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
+                 return st ? efm_launch_stream(EFM_ADJ, 1, ctx->rows, ctx->ring, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s)
+                           : efm_launch_velocity(EFM_ADJ, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s);
+             })))
+            return rc;
+        if (model) {
+            const int kv = (it & 1) ? T_REV_V1 : T_REV_V0, ks = (it & 1) ? T_REV_S1 : T_REV_S0;
+            const int ki = (it & 1) ? T_IMG1 : T_IMG0;
+            // stream kernels: rebuild, then imaging; otherwise one fused rebuild + imaging kernel
+            if ((rc = timed_launch(ctx, EFM_K_REV_VELOCITY, s, [&] {
+                     return st ? efm_launch_stream(EFM_REV, 1, ctx->rows, ctx->ring, dtab(kv), n, ctx->tiles[kv], it, s)
+                               : efm_launch_velocity(EFM_REV, dtab(kv), n, ctx->tiles[kv], it, s);
+                 })))
+                return rc;
+            if (st && (rc = timed_launch(ctx, EFM_K_IMAGING, s, [&] {
+                           return efm_launch_image(dtab(ki), n, ctx->tiles[ki], it, s);
+                       })))
+                return rc;
+            if ((rc = timed_launch(ctx, EFM_K_REV_STRESS, s, [&] {
+                     return st ? efm_launch_stream(EFM_REV, 0, ctx->rows, ctx->ring, dtab(ks), n, ctx->tiles[ks], it, s)
+                               : efm_launch_stress(EFM_REV, dtab(ks), n, ctx->tiles[ks], it, s);
+                 })))
+                return rc;
+        }
+    }
+    return EFM_OK;
+}
+
 }  // namespace
 
 // ============================================================================ C ABI
@@ -750,12 +873,15 @@ int efm_clear(efm_ctx *ctx) {
     for (Inst &I : ctx->inst) free_inst(I);
     ctx->inst.clear();
     ctx->layout_ready = false;
+    drop_loops(ctx);
     return EFM_OK;
 }
 
 int efm_destroy(efm_ctx *ctx) {
     if (ctx == nullptr) return EFM_OK;
     efm_clear(ctx);
+    drop_loops(ctx);
+    if (ctx->cap_stream != nullptr) cudaStreamDestroy(ctx->cap_stream);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     cudaFree(ctx->d_maps);
     cudaFree(ctx->d_err);
@@ -930,19 +1056,32 @@ int efm_forward(efm_ctx *ctx, float *gathers, int save, void *stream) {
         I.fwd_saved = false;
         I.ck_saved = false;
     }
-    for (int it = 0; it < maxnt; ++it) {
-        if ((rc = forward_step(ctx, st, it, s))) return rc;
-        if (ckpts)
-            for (Inst &I : ctx->inst)
-                if ((it + 1) % I.ck_every == 0 && it + 1 < I.nt) {
-                    // checkpoint k = (it+1)/K holds the state after step it (k >= 1; 0 = zeros)
-                    float *dst = I.ckpt + (size_t)((it + 1) / I.ck_every - 1) * ckpt_floats(I);
-                    EFM_CK(cudaMemcpyAsync(dst, I.fields, 9 * I.ncell * sizeof(float),
-                                           cudaMemcpyDeviceToDevice, s));
-                    EFM_CK(cudaMemcpyAsync(dst + 9 * I.ncell, I.psi, psi_floats(I) * sizeof(float),
-                                           cudaMemcpyDeviceToDevice, s));
-                }
-    }
+    std::vector<int64_t> key = {st, ctx->rows, ctx->ring, ctx->opt_pdl, (int64_t)ctx->inst.size(),
+                                maxnt, (int64_t)(uintptr_t)ctx->d_tab, ctx->tiles[T_FWD_S],
+                                ctx->tiles[T_FWD_V], ckpts};
+    if (ckpts)
+        for (const Inst &I : ctx->inst)
+            key.insert(key.end(), {I.ck_every, I.nt, (int64_t)(uintptr_t)I.ckpt,
+                                   (int64_t)(uintptr_t)I.fields, (int64_t)(uintptr_t)I.psi,
+                                   I.ncell, (int64_t)psi_floats(I)});
+    rc = run_loop(ctx, 0, key, s, [&](cudaStream_t ls) {
+        int r;
+        for (int it = 0; it < maxnt; ++it) {
+            if ((r = forward_step(ctx, st, it, ls))) return r;
+            if (ckpts)
+                for (Inst &I : ctx->inst)
+                    if ((it + 1) % I.ck_every == 0 && it + 1 < I.nt) {
+                        // checkpoint k = (it+1)/K holds the state after step it (k >= 1; 0 = zeros)
+                        float *dst = I.ckpt + (size_t)((it + 1) / I.ck_every - 1) * ckpt_floats(I);
+                        EFM_CK(cudaMemcpyAsync(dst, I.fields, 9 * I.ncell * sizeof(float),
+                                               cudaMemcpyDeviceToDevice, ls));
+                        EFM_CK(cudaMemcpyAsync(dst + 9 * I.ncell, I.psi, psi_floats(I) * sizeof(float),
+                                               cudaMemcpyDeviceToDevice, ls));
+                    }
+        }
+        return (int)EFM_OK;
+    });
+    if (rc) return rc;
     for (Inst &I : ctx->inst) {
         I.fwd_saved = strips;
         I.ck_saved = ckpts;
@@ -1110,61 +1249,11 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                      return efm_launch_reciprocals(I.mu, I.rho, I.aux, I.aux + I.ncell, I.ncell, s);
                  })))
                 return rc;
-    auto dtab = [&](int k) { return (const EfmInst *)(ctx->d_tab + (size_t)k * n); };
-    for (int it = 0; it < maxsteps; ++it) {
-        if (st && model && ctx->opt_pair) {
-            // (adjoint stress | rebuild velocity), (rebuild stress | adjoint velocity), imaging:
-            // within a step the adjoint chain and the rebuild write disjoint fields, and the
-            // imaging reads neither the rebuild's stress nor anything the next step's first
-            // pair writes before this step's imaging has finished (stream order)
-            const int kv = (it & 1) ? T_REV_V1 : T_REV_V0, ks = (it & 1) ? T_REV_S1 : T_REV_S0;
-            const int ki = (it & 1) ? T_IMG1 : T_IMG0;
-            if ((rc = timed_launch(ctx, EFM_K_PAIR_ADJS_REVV, s, [&] {
-                     return efm_launch_pair(0, ctx->rows, ctx->ring, dtab(T_ADJ_S), ctx->tiles[T_ADJ_S],
-                                            dtab(kv), ctx->tiles[kv], n, it, s);
-                 })))
-                return rc;
-            if ((rc = timed_launch(ctx, EFM_K_PAIR_REVS_ADJV, s, [&] {
-                     return efm_launch_pair(1, ctx->rows, ctx->ring, dtab(ks), ctx->tiles[ks],
-                                            dtab(T_ADJ_V), ctx->tiles[T_ADJ_V], n, it, s);
-                 })))
-                return rc;
-            if ((rc = timed_launch(ctx, EFM_K_IMAGING, s, [&] {
-                     return efm_launch_image(dtab(ki), n, ctx->tiles[ki], it, s);
-                 })))
-                return rc;
-            continue;
-        }
-        if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
-                 return st ? efm_launch_stream(EFM_ADJ, 0, ctx->rows, ctx->ring, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s)
-                           : efm_launch_stress(EFM_ADJ, dtab(T_ADJ_S), n, ctx->tiles[T_ADJ_S], it, s);
-             })))
-            return rc;
-        if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
-                 return st ? efm_launch_stream(EFM_ADJ, 1, ctx->rows, ctx->ring, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s)
-                           : efm_launch_velocity(EFM_ADJ, dtab(T_ADJ_V), n, ctx->tiles[T_ADJ_V], it, s);
-             })))
-            return rc;
-        if (model) {
-            const int kv = (it & 1) ? T_REV_V1 : T_REV_V0, ks = (it & 1) ? T_REV_S1 : T_REV_S0;
-            const int ki = (it & 1) ? T_IMG1 : T_IMG0;
-            // stream kernels: rebuild, then imaging; otherwise one fused rebuild + imaging kernel
-            if ((rc = timed_launch(ctx, EFM_K_REV_VELOCITY, s, [&] {
-                     return st ? efm_launch_stream(EFM_REV, 1, ctx->rows, ctx->ring, dtab(kv), n, ctx->tiles[kv], it, s)
-                               : efm_launch_velocity(EFM_REV, dtab(kv), n, ctx->tiles[kv], it, s);
-                 })))
-                return rc;
-            if (st && (rc = timed_launch(ctx, EFM_K_IMAGING, s, [&] {
-                           return efm_launch_image(dtab(ki), n, ctx->tiles[ki], it, s);
-                       })))
-                return rc;
-            if ((rc = timed_launch(ctx, EFM_K_REV_STRESS, s, [&] {
-                     return st ? efm_launch_stream(EFM_REV, 0, ctx->rows, ctx->ring, dtab(ks), n, ctx->tiles[ks], it, s)
-                               : efm_launch_stress(EFM_REV, dtab(ks), n, ctx->tiles[ks], it, s);
-                 })))
-                return rc;
-        }
-    }
+    std::vector<int64_t> key = {st, model, ctx->opt_pair, ctx->rows, ctx->ring, ctx->opt_pdl, n,
+                                maxsteps, (int64_t)(uintptr_t)ctx->d_tab};
+    key.insert(key.end(), ctx->tiles + T_ADJ_S, ctx->tiles + T_NSLOT);
+    rc = run_loop(ctx, 1, key, s, [&](cudaStream_t ls) { return gradient_loop(ctx, st, model, n, maxsteps, ls); });
+    if (rc) return rc;
     if (model)
         for (Inst &I : ctx->inst) I.fwd_saved = false;  // the rebuild consumed the forward state
     return EFM_OK;
@@ -1189,6 +1278,7 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             break;
         case EFM_OPT_PAIR_LAUNCH: ctx->opt_pair = value != 0; break;
         case EFM_OPT_PDL: ctx->opt_pdl = value != 0; break;
+        case EFM_OPT_GRAPH: ctx->opt_graph = value != 0; break;
         case EFM_OPT_RING_DEPTH:
             if (value != 0 && value != 4 && value != 6) return fail(EFM_ERR_ARG, "ring depth must be 0, 4 or 6");
             ctx->opt_ring = value;

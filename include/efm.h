@@ -201,6 +201,11 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 /* 1 (default): launch the plane-streaming kernels as programmatic dependents, so each one's
  * prologue overlaps the tail of the previous kernel; 0: plain stream order. */
 #define EFM_OPT_PDL 7
+/* 1 (default): the time loops of efm_forward and efm_gradient are captured once as a CUDA
+ * graph and replayed on the caller's stream while the tables, grid sizes and options stay
+ * the same (kernel counters still count every launch); 0: launched step by step.  Loops
+ * run with efm_set_timing(ctx, 1) are always launched step by step. */
+#define EFM_OPT_GRAPH 8
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*

@@ -340,3 +340,34 @@ def test_paired_gradient_launches_equal_sequential(golden_c1scale, cuda, rows, r
         out.append((g.cpu().numpy(), m.cpu().numpy()))
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_graph_replay_equals_step_launches(golden_c1scale, cuda):
+    """Time loops captured as CUDA graphs and replayed (twice, the second call a pure replay)
+    give bit-identical gathers, gradients and checkpointed states to step-by-step launches,
+    and the kernel counters count the replayed launches."""
+    import ctypes
+
+    from elastic_fm_vp_vs_rho_b200 import _lib
+    d = golden_c1scale
+    L = _lib.load()
+    out = {}
+    for graph in (1, 0):
+        b = _batch(d, d["lam0"], d["mu0"], d["rho0"], d["mt_obs"])
+        b.set_option(_lib.EFM_OPT_GRAPH, graph)
+        runs = []
+        for _ in range(2):
+            _lib.check(L.efm_kernel_stats(b._ctx, None, None, 1))
+            mod = b.forward(save_borders=True)
+            res, _ = b.residual_misfit(mod, cuda.as_tensor(d["obs0"].reshape(-1)).cuda())
+            g, m = b.gradient(res, model=True, mt=True)
+            b.status()
+            n = (ctypes.c_int64 * _lib.EFM_NKERN)()
+            _lib.check(L.efm_kernel_stats(b._ctx, n, None, 1))
+            runs.append((mod.cpu().numpy(), g.cpu().numpy(), m.cpu().numpy(), list(n)))
+        for a, c in zip(*runs):
+            assert np.array_equal(np.asarray(a), np.asarray(c))
+        out[graph] = runs[0]
+    for a, c in zip(out[1], out[0]):
+        assert np.array_equal(np.asarray(a), np.asarray(c))
+    assert out[1][3][0] == int(d["nt"])  # EFM_K_FWD_STRESS: one launch per step

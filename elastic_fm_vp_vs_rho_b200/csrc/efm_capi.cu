@@ -174,8 +174,9 @@ struct efm_ctx {
 enum { T_FWD_S, T_FWD_V, T_ADJ_S, T_ADJ_V, T_REV_V0, T_REV_V1, T_REV_S0, T_REV_S1, T_IMG0,
        T_IMG1, T_NSLOT };
 // tensor-map blocks per instance
+// (the rebuild velocity's block ends with the three maps its new velocity is stored through)
 enum { M_FWD_S = 0, M_FWD_V = 11, M_ADJ_S = 21, M_ADJ_V = 32, M_REV_S0 = 42, M_REV_S1 = 53,
-       M_REV_V0 = 64, M_REV_V1 = 74, M_IMG0 = 84, M_IMG1 = 104, EFM_MAPS_PER_INST = 128 };
+       M_REV_V0 = 64, M_REV_V1 = 77, M_IMG0 = 90, M_IMG1 = 110, EFM_MAPS_PER_INST = 130 };
 #define EFM_IMG_TZ 4
 static_assert(T_NSLOT <= 16, "efm_ctx::tiles holds 16 table slots");
 
@@ -1201,9 +1202,10 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
                 // reverse velocity rebuild: the velocity pass's fields, old velocity in f.v
                 layout_stream(rv, yc, tz);
                 const int mv = p == 0 ? M_REV_V0 : M_REV_V1;
-                const float *vf[10] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
-                                       I.tt(1), r.f.v[0], r.f.v[1], r.f.v[2]};
-                for (int q = 0; q < 10; ++q)
+                const float *vf[13] = {I.tt(0), I.tt(2), I.tt(3), I.tt(4), I.tt(5), I.aux + I.ncell,
+                                       I.tt(1), r.f.v[0], r.f.v[1], r.f.v[2], r.f.vo[0], r.f.vo[1],
+                                       r.f.vo[2]};
+                for (int q = 0; q < 13; ++q)
                     if ((rc = encode_map(m + mv + q, vf[q], I, q < 6 ? EFM_HX : EFM_STX,
                                          q < 6 ? hz : tz)))
                         return rc;

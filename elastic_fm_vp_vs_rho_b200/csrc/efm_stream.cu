@@ -14,9 +14,16 @@
 // built on the host), reciprocals of mu and rho come precomputed, and one block barrier
 // per plane both frees the oldest stage and makes a timed-out wait end every thread's loop.
 //
+// Each thread writes its new values over the old ones in the plane's stage (cell fields are
+// read only by their own thread); after the barrier one thread stores the plane's updated
+// fields with TMA tile stores (one bulk group per plane) and refills the oldest stage once
+// the store out of it has been read.  The per-cell work is then shared-memory loads, the
+// arithmetic and shared-memory stores; global addresses are formed only for the CPML memory
+// variables (offsets hoisted per thread row, plane bases per plane), receivers and strips.
+//
 // Arithmetic, guards, CPML, sources, receivers, strips and MT strain follow efm_stencil.cu
 // (kernel_Tau :59-128, kernel_Vx_Vy_Vz :133-188 of mainPropElastic3D_MT.py); harmonic means
-// use the hardware reciprocal (relative error ~1 ulp).  Outputs are coalesced plain stores.
+// use the hardware reciprocal (relative error ~1 ulp).
 #include "efm_internal.cuh"
 #include "efm_stream.cuh"
 #include "efm_tma.cuh"
@@ -32,18 +39,19 @@ __device__ __forceinline__ float frcp(float a) {
 template <int ROWS, int SR>
 struct Ring {
     static constexpr int HB = efm_halo_bytes(ROWS), CB = efm_center_bytes(ROWS);
+    static constexpr int CF = CB / 4;  // floats per cell field
     unsigned char *base;
     uint64_t *bar;
     int stage_bytes;
     int nh;
-    int p0;  // plane held by stage 0 at its first use
-    __device__ __forceinline__ int stage(int p) const { return (p - p0) % SR; }
-    __device__ __forceinline__ uint32_t parity(int p) const { return ((p - p0) / SR) & 1; }
+    int p0;  // plane held by stage 0 at its first use (planes only grow from p0)
+    __device__ __forceinline__ int stage(int p) const { return (int)((unsigned)(p - p0) % SR); }
+    __device__ __forceinline__ uint32_t parity(int p) const { return ((unsigned)(p - p0) / SR) & 1u; }
     __device__ __forceinline__ const float *halo(int s, int f) const {
         return reinterpret_cast<const float *>(base + s * stage_bytes + f * HB);
     }
-    __device__ __forceinline__ const float *center(int s, int f) const {
-        return reinterpret_cast<const float *>(base + s * stage_bytes + nh * HB + f * CB);
+    __device__ __forceinline__ float *center(int s, int f) const {
+        return reinterpret_cast<float *>(base + s * stage_bytes + nh * HB + f * CB);
     }
 };
 
@@ -61,6 +69,25 @@ __device__ __forceinline__ void issue_plane(const Ring<ROWS, SR> &R, const CUten
 #pragma unroll
     for (int f = 0; f < NC; ++f)
         efm_tma_load_3d(st + NH * HB + f * CB, tm + NH + f, bar, x0, z0, p);
+}
+
+// End of plane j, thread 0, after the block barrier: store the n updated cell fields
+// [f0, f0 + n) of plane j's stage through the maps sm[0 .. n) (when `store`), close plane j's
+// bulk group, and refill the stage of plane j-1 with plane j-1+SR once the store out of it
+// (closed one plane earlier) has finished reading it.
+template <int ROWS, int SR, int NH, int NC>
+__device__ __forceinline__ void advance(const Ring<ROWS, SR> &R, const CUtensorMap *tm,
+                                        const CUtensorMap *sm, int f0, int n, bool store, int x0,
+                                        int z0, int j, int last) {
+    if (store) {
+        const int s = R.stage(j);
+        for (int f = 0; f < n; ++f) efm_tma_store_3d(sm + f, R.center(s, f0 + f), x0, z0, j);
+    }
+    efm_bulk_commit();
+    if (j - 1 + SR <= last) {
+        efm_bulk_wait_read<1>();
+        issue_plane<ROWS, SR, NH, NC>(R, tm, x0, z0, j - 1 + SR);
+    }
 }
 
 struct Tile {
@@ -130,45 +157,100 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
     }
 }
 
+// Per-block constants of the plane loop, read from the instance table once.  The loop's
+// mbarrier waits are asm statements with a memory clobber, after which the compiler would
+// otherwise reload every table field it touches.  The memory variables of a pass are three
+// consecutive components of each slab family (FIRST 0: stress, 3: velocity).
+struct Hot {
+    float *psx, *psy, *psz;  // component FIRST of each family
+    int64_t stx, sty, stz;   // component strides
+    int64_t pxs, pys, pzs;   // plane strides: nz*2W (x slabs), nz*nx (y slabs), W*nx (z slab)
+    float k;
+    int nx, ny, nz, W;
+};
+
+__device__ __forceinline__ Hot make_hot(const EfmInst &I, int first) {
+    Hot h;
+    h.nx = I.nx;
+    h.ny = I.ny;
+    h.nz = I.nz;
+    h.W = I.W;
+    h.stx = (int64_t)I.ny * I.nz * 2 * I.W;
+    h.sty = (int64_t)2 * I.W * I.nz * I.nx;
+    h.stz = (int64_t)I.ny * I.W * I.nx;
+    h.pxs = (int64_t)I.nz * 2 * I.W;
+    h.pys = (int64_t)I.nz * I.nx;
+    h.pzs = (int64_t)I.W * I.nx;
+    h.psx = I.psi_x + first * h.stx;
+    h.psy = I.psi_y + first * h.sty;
+    h.psz = I.psi_z + first * h.stz;
+    h.k = I.k;
+    return h;
+}
+
+// One thread row (cells (x, z0 + r + 4h) of every plane): ring indices, whether the stencil
+// updates it, and its memory-variable offsets inside a plane of each slab family (-1: none).
+struct Row {
+    int hidx, cidx;
+    int pxo, pyo, pzo;
+    bool in;
+};
+
+// Memory-variable rows of one plane (component FIRST; y null outside the y slabs).
+struct PsiPlane {
+    float *x, *y, *z;
+};
+
+__device__ __forceinline__ PsiPlane psi_plane(const Hot &H, int y) {
+    PsiPlane P;
+    P.x = H.psx + (int64_t)y * H.pxs;
+    P.z = H.psz + (int64_t)y * H.pzs;
+    P.y = nullptr;
+    if (y < H.W) P.y = H.psy + (int64_t)y * H.pys;
+    else if (y >= H.ny - H.W) P.y = H.psy + (int64_t)(y - (H.ny - 2 * H.W)) * H.pys;
+    return P;
+}
+
+// Request the 9 old memory variables of one cell (zeros where it has none): 0-2 x family,
+// 3-5 y family, 6-8 z family.
+__device__ __forceinline__ void load_psi(const Hot &H, const PsiPlane &P, const Row &r, float *pp) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) pp[q] = 0.f;
+    if (r.pxo >= 0) {
+        const float *p = P.x + r.pxo;
+        pp[0] = p[0];
+        pp[1] = p[H.stx];
+        pp[2] = p[2 * H.stx];
+    }
+    if (P.y != nullptr) {
+        const float *p = P.y + r.pyo;
+        pp[3] = p[0];
+        pp[4] = p[H.sty];
+        pp[5] = p[2 * H.sty];
+    }
+    if (r.pzo >= 0) {
+        const float *p = P.z + r.pzo;
+        pp[6] = p[0];
+        pp[7] = p[H.stz];
+        pp[8] = p[2 * H.stz];
+    }
+}
+
 // ------------------------------------------------------------------------------ stress
 // CPML coefficients of one cell, loaded once per block (x, z) or per plane (y)
 struct Coef {
     float ax, bx, ay, by, az, bz;
 };
 
-// Per-block constants of the plane loop, read from the instance table once.  The loop's
-// mbarrier waits are asm statements with a memory clobber, after which the compiler would
-// otherwise reload every table field it touches; the fields of a pass are consecutive
-// volumes of one allocation, so one base pointer and the volume size address all of them.
-struct Hot {
-    float *out;       // first output volume: txx (stress) or vx (velocity / rebuild target)
-    float *psx, *psy, *psz;
-    int64_t nc;       // cells per volume
-    float k;
-    int nx, ny, nz, W;
-};
-
-__device__ __forceinline__ Hot make_hot(const EfmInst &I, float *out) {
-    Hot h;
-    h.out = out;
-    h.psx = I.psi_x;
-    h.psy = I.psi_y;
-    h.psz = I.psi_z;
-    h.nc = (int64_t)I.nx * I.ny * I.nz;
-    h.k = I.k;
-    h.nx = I.nx;
-    h.ny = I.ny;
-    h.nz = I.nz;
-    h.W = I.W;
-    return h;
-}
-
+// New stress of one cell, written over its old stress in the ring (the block stores the
+// plane with TMA afterwards).
 template <int PASS, int ROWS, int SR>
 __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, SR> &R, int sm, int s0,
-                                            int sp, int it, int x, int y, int z, int hidx,
-                                            int cidx, bool has_src, const float *pp, const Coef &C,
-                                            const Hot &H) {
-    const int nx = H.nx, ny = H.ny, nz = H.nz, W = H.W;
+                                            int sp, int it, int x, int y, int z, const Row &rw,
+                                            bool has_src, const float *pp, const Coef &C,
+                                            const Hot &H, const PsiPlane &P) {
+    constexpr int CF = Ring<ROWS, SR>::CF;
+    const int hidx = rw.hidx;
     const float *vx0 = R.halo(s0, 0), *vy0 = R.halo(s0, 1), *vz0 = R.halo(s0, 2);
     const float *rm0 = R.halo(s0, 3), *rm1 = R.halo(sp, 3);
     const float vxc = vx0[hidx], vyc = vy0[hidx], vzc = vz0[hidx];
@@ -185,41 +267,35 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
     float pvz_z = 0.f, pvx_z = 0.f, pvy_z = 0.f;
     if (PASS != EFM_REV) {
         // pp: the 9 old memory variables requested at the top of the iteration
-        if (x < W || x >= nx - W) {
-            const int xs = x < W ? x : x - (nx - 2 * W);
-            const int64_t st = (int64_t)ny * nz * 2 * W;
-            float *p = H.psx + ((int64_t)y * nz + z) * (2 * W) + xs;
+        if (rw.pxo >= 0) {
+            float *p = P.x + rw.pxo;
             const float a = C.ax, b = C.bx;
             pvx_x = b * pp[0] + a * dvx_dx;
             pvy_x = b * pp[1] + a * dvy_dx;
             pvz_x = b * pp[2] + a * dvz_dx;
             p[0] = pvx_x;
-            p[st] = pvy_x;
-            p[2 * st] = pvz_x;
+            p[H.stx] = pvy_x;
+            p[2 * H.stx] = pvz_x;
         }
-        if (y < W || y >= ny - W) {
-            const int ys = y < W ? y : y - (ny - 2 * W);
-            const int64_t st = (int64_t)2 * W * nz * nx;
-            float *p = H.psy + ((int64_t)ys * nz + z) * nx + x;
+        if (P.y != nullptr) {
+            float *p = P.y + rw.pyo;
             const float a = C.ay, b = C.by;
             pvy_y = b * pp[3] + a * dvy_dy;
             pvx_y = b * pp[4] + a * dvx_dy;
             pvz_y = b * pp[5] + a * dvz_dy;
             p[0] = pvy_y;
-            p[st] = pvx_y;
-            p[2 * st] = pvz_y;
+            p[H.sty] = pvx_y;
+            p[2 * H.sty] = pvz_y;
         }
-        if (z >= nz - W) {
-            const int zs = z - (nz - W);
-            const int64_t st = (int64_t)ny * W * nx;
-            float *p = H.psz + ((int64_t)y * W + zs) * nx + x;
+        if (rw.pzo >= 0) {
+            float *p = P.z + rw.pzo;
             const float a = C.az, b = C.bz;
             pvz_z = b * pp[6] + a * dvz_dz;
             pvx_z = b * pp[7] + a * dvx_dz;
             pvy_z = b * pp[8] + a * dvy_dz;
             p[0] = pvz_z;
-            p[st] = pvx_z;
-            p[2 * st] = pvy_z;
+            p[H.stz] = pvx_z;
+            p[2 * H.stz] = pvy_z;
         }
     }
     // harmonic 4-point averages of mu from the precomputed 1/mu (:80-89)
@@ -230,15 +306,16 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
     const float mu_xz = 4.f * frcp(r0 + ri + rk + rik);
     const float mu_xy = 4.f * frcp(r0 + ri + rj + rij);
     const float mu_yz = 4.f * frcp(r0 + rj + rk + rjk);
-    const float lam = R.center(s0, 0)[cidx];
+    float *cw = R.center(s0, 0) + rw.cidx;  // lambda, then txx tyy tzz txy txz tyz
+    const float lam = cw[0];
     const float k = H.k;
     const float l2m = lam + 2.f * mu0;
-    float txx = R.center(s0, 1)[cidx] + k * (l2m * (dvx_dx + pvx_x) + lam * (dvy_dy + dvz_dz + pvy_y + pvz_z));
-    float tyy = R.center(s0, 2)[cidx] + k * (l2m * (dvy_dy + pvy_y) + lam * (dvx_dx + dvz_dz + pvx_x + pvz_z));
-    float tzz = R.center(s0, 3)[cidx] + k * (l2m * (dvz_dz + pvz_z) + lam * (dvx_dx + dvy_dy + pvx_x + pvy_y));
-    float txy = R.center(s0, 4)[cidx] + k * mu_xy * ((dvx_dy + pvx_y) + (dvy_dx + pvy_x));
-    float txz = R.center(s0, 5)[cidx] + k * mu_xz * ((dvx_dz + pvx_z) + (dvz_dx + pvz_x));
-    float tyz = R.center(s0, 6)[cidx] + k * mu_yz * ((dvy_dz + pvy_z) + (dvz_dy + pvz_y));
+    float txx = cw[CF] + k * (l2m * (dvx_dx + pvx_x) + lam * (dvy_dy + dvz_dz + pvy_y + pvz_z));
+    float tyy = cw[2 * CF] + k * (l2m * (dvy_dy + pvy_y) + lam * (dvx_dx + dvz_dz + pvx_x + pvz_z));
+    float tzz = cw[3 * CF] + k * (l2m * (dvz_dz + pvz_z) + lam * (dvx_dx + dvy_dy + pvx_x + pvy_y));
+    float txy = cw[4 * CF] + k * mu_xy * ((dvx_dy + pvx_y) + (dvy_dx + pvy_x));
+    float txz = cw[5 * CF] + k * mu_xz * ((dvx_dz + pvx_z) + (dvz_dx + pvz_x));
+    float tyz = cw[6 * CF] + k * mu_yz * ((dvy_dz + pvy_z) + (dvz_dy + pvz_y));
     if (PASS != EFM_ADJ && has_src) {
         const int widx = (PASS == EFM_FWD) ? it : I.nt - 1 - it;
         for (int s = 0; s < I.nsrc; ++s) {
@@ -254,14 +331,12 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
             }
         }
     }
-    const int64_t c = x + (int64_t)nx * (z + (int64_t)nz * y);
-    float *o = H.out + c;
-    o[0] = txx;
-    o[H.nc] = tyy;
-    o[2 * H.nc] = tzz;
-    o[3 * H.nc] = txy;
-    o[4 * H.nc] = txz;
-    o[5 * H.nc] = tyz;
+    cw[CF] = txx;
+    cw[2 * CF] = tyy;
+    cw[3 * CF] = tzz;
+    cw[4 * CF] = txy;
+    cw[5 * CF] = txz;
+    cw[6 * CF] = tyz;
     if (PASS == EFM_ADJ && has_src && I.mtg != nullptr) {
         for (int s = 0; s < I.nsrc; ++s) {
             if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s]) {
@@ -280,37 +355,46 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
     }
 }
 
-// Request the 9 old CPML memory variables of one cell (zeros where the cell has none).
-template <int FIRST>
-__device__ __forceinline__ void load_psi(const EfmInst &I, const Hot &H, int x, int y, int z,
-                                         float *pp) {
-    const int nx = H.nx, ny = H.ny, nz = H.nz, W = H.W;
+// Row constants of the thread's cells (x, z0 + lr + 4h).
+template <int PASS, int ROWS>
+__device__ __forceinline__ void make_rows(const Hot &H, const Tile &T, int x, int lx, int lr,
+                                          bool stress, Row *rw) {
+    const int nx = H.nx, nz = H.nz, W = H.W;
+    const bool xpml = x < nx && (x < W || x >= nx - W);
+    const int xs = x < W ? x : x - (nx - 2 * W);
 #pragma unroll
-    for (int q = 0; q < 9; ++q) pp[q] = 0.f;
-    if (x < W || x >= nx - W) {
-        const int xs = x < W ? x : x - (nx - 2 * W);
-        const int64_t st = (int64_t)ny * nz * 2 * W;
-        const float *p = H.psx + FIRST * st + ((int64_t)y * nz + z) * (2 * W) + xs;
-        pp[0] = p[0];
-        pp[1] = p[st];
-        pp[2] = p[2 * st];
+    for (int h = 0; h < ROWS; ++h) {
+        const int lz = lr + 4 * h, z = T.z0 + lz;
+        rw[h].hidx = (lz + 1) * EFM_HX + lx + EFM_HX_OFF;
+        rw[h].cidx = lz * EFM_STX + lx;
+        rw[h].in = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS &&
+                   !(stress && PASS == EFM_REV && (x < W || x >= nx - W || z >= nz - W));
+        rw[h].pxo = xpml && z < nz ? z * 2 * W + xs : -1;
+        rw[h].pyo = z * nx + x;
+        rw[h].pzo = z < nz && z >= nz - W && x < nx ? (z - (nz - W)) * nx + x : -1;
     }
-    if (y < W || y >= ny - W) {
-        const int ys = y < W ? y : y - (ny - 2 * W);
-        const int64_t st = (int64_t)2 * W * nz * nx;
-        const float *p = H.psy + FIRST * st + ((int64_t)ys * nz + z) * nx + x;
-        pp[3] = p[0];
-        pp[4] = p[st];
-        pp[5] = p[2 * st];
-    }
-    if (z >= nz - W) {
-        const int zs = z - (nz - W);
-        const int64_t st = (int64_t)ny * W * nx;
-        const float *p = H.psz + FIRST * st + ((int64_t)y * W + zs) * nx + x;
-        pp[6] = p[0];
-        pp[7] = p[st];
-        pp[8] = p[2 * st];
-    }
+}
+
+// Boundary-strip slots of one thread row (efm_strip_slots_v with the plane terms split off):
+// X faces xf + yr*bz, Y faces yf + row*bz*bx on the two planes next to each y face of the box,
+// Z faces zf + yr*bx; -1 where the row owns no slot of that family (yf < 0: (x, z) outside the
+// box).
+struct StripRow {
+    int xf, yf, zf;
+};
+
+__device__ __forceinline__ StripRow strip_row(int nx, int nz, int by, int W, int x, int z) {
+    const int bx = nx - 2 * W, bz = nz - W - 2;
+    const int xr = x - W, zr = z - 2;
+    StripRow s{-1, -1, -1};
+    if (xr < 0 || xr >= bx || zr < 0 || zr >= bz) return s;
+    const int offY = 4 * by * bz, offZ = offY + 4 * bz * bx;
+    const int col = xr < 2 ? xr : (xr >= bx - 2 ? 2 + (xr - (bx - 2)) : -1);
+    if (col >= 0) s.xf = col * by * bz + zr;
+    s.yf = offY + zr * bx + xr;
+    const int pl = zr < 2 ? zr : (zr >= bz - 2 ? 2 + (zr - (bz - 2)) : -1);
+    if (pl >= 0) s.zf = offZ + pl * by * bx + xr;
+    return s;
 }
 
 }  // namespace
@@ -334,19 +418,15 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const bool has_src = s_src != 0;
-    const Hot H = make_hot(I, I.f.t[0]);
-    bool colin[ROWS];
-    int hidx[ROWS], cidx[ROWS];
+    const Hot H = make_hot(I, 0);
+    Row rw[ROWS];
+    make_rows<PASS, ROWS>(H, T, x, lx, lr, true, rw);
     Coef cf[ROWS];
     const bool xpml = x < nx && (x < W || x >= nx - W);
     const float cx_a = xpml ? I.cpml[x] : 0.f, cx_b = xpml ? I.cpml[nx + x] : 0.f;
 #pragma unroll
     for (int h = 0; h < ROWS; ++h) {
-        const int lz = lr + 4 * h, z = T.z0 + lz;
-        hidx[h] = (lz + 1) * EFM_HX + lx + EFM_HX_OFF;
-        cidx[h] = lz * EFM_STX + lx;
-        colin[h] = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS &&
-                   !(PASS == EFM_REV && (x < W || x >= nx - W || z >= nz - W));
+        const int z = T.z0 + lr + 4 * h;
         const bool zpml = z < nz && z >= nz - W;
         cf[h].ax = cx_a;
         cf[h].bx = cx_b;
@@ -370,36 +450,41 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
             cf[h].ay = cy_a;
             cf[h].by = cy_b;
         }
+        PsiPlane P{nullptr, nullptr, nullptr};
         float pp[ROWS][9];
         if (PASS != EFM_REV) {
+            P = psi_plane(H, j);
 #pragma unroll
             for (int h = 0; h < ROWS; ++h)
-                if (plane_in && colin[h]) load_psi<0>(I, H, x, j, T.z0 + lr + 4 * h, pp[h]);
+                if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
         }
         const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
         if (mine && plane_in) {
             const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
             for (int h = 0; h < ROWS; ++h)
-                if (colin[h])
-                    stress_cell<PASS, ROWS, SR>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, hidx[h],
-                                      cidx[h], has_src, pp[h], cf[h], H);
+                if (rw[h].in)
+                    stress_cell<PASS, ROWS, SR>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, rw[h],
+                                                has_src, pp[h], cf[h], H, P);
+            efm_fence_async_smem();
         }
         ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
         if (!ok) break;
-        if (j - 1 + SR <= last) {
-            if (threadIdx.x == 0) issue_plane<ROWS, SR, NH, NC>(R, tm, T.x0, T.z0, j - 1 + SR);
-            issued_hi = j - 1 + SR;
-        }
+        if (threadIdx.x == 0)
+            advance<ROWS, SR, NH, NC>(R, tm, tm + NH + 1, 1, 6, plane_in, T.x0, T.z0, j, last);
+        if (j - 1 + SR <= last) issued_hi = j - 1 + SR;
     }
+    if (threadIdx.x == 0) efm_bulk_wait_all();
     if (!ok) drain(R, R.p0, issued_hi);  // no load may still target this block's smem
 }
 
-// halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint)
+// halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint);
+// the rebuild stores its new velocity through three more maps (tm[NH + NC ..]) into f.vo
 template <int PASS, int ROWS, int SR>
 __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts, int ninst, int it,
                                               int block, unsigned char *smem) {
     constexpr int NH = 6, NC = 4;
+    constexpr int CF = Ring<ROWS, SR>::CF;
     __shared__ uint64_t bars[SR];
     __shared__ int s_src;
     __shared__ unsigned long long s_rec;
@@ -414,25 +499,28 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const unsigned long long recbits = s_rec;
-    const Hot H = make_hot(I, PASS == EFM_REV ? I.f.vo[0] : I.f.v[0]);
+    const Hot H = make_hot(I, 3);
     float *const border = I.border;
     const int64_t strip_n = I.strip_n;
-    bool colin[ROWS], colgrid[ROWS];
-    int hidx[ROWS], cidx[ROWS];
+    const int by = ny - 2 * W, bx = nx - 2 * W, bz = nz - W - 2;
+    Row rw[ROWS];
+    make_rows<PASS, ROWS>(H, T, x, lx, lr, false, rw);
+    StripRow sr[ROWS];
+    bool colgrid[ROWS], zone_xz[ROWS];
     float cz_a[ROWS], cz_b[ROWS];
     const bool xpml = x < nx && (x < W || x >= nx - W);
     const float cx_a = xpml ? I.cpml[x] : 0.f, cx_b = xpml ? I.cpml[nx + x] : 0.f;
 #pragma unroll
     for (int h = 0; h < ROWS; ++h) {
-        const int lz = lr + 4 * h, z = T.z0 + lz;
-        hidx[h] = (lz + 1) * EFM_HX + lx + EFM_HX_OFF;
-        cidx[h] = lz * EFM_STX + lx;
-        colin[h] = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS;
+        const int z = T.z0 + lr + 4 * h;
         colgrid[h] = x < nx && z < nz;
+        zone_xz[h] = x < W || x >= nx - W || z >= nz - W;
+        sr[h] = strip_row(nx, nz, by, W, x, z);
         const bool zpml = z < nz && z >= nz - W;
         cz_a[h] = zpml ? I.cpml[2 * nx + 2 * ny + z] : 0.f;
         cz_b[h] = zpml ? I.cpml[2 * nx + 2 * ny + nz + z] : 0.f;
     }
+    const CUtensorMap *stm = PASS == EFM_REV ? tm + NH + NC : tm + NH + 1;
     const int last = T.ye;
     int issued_hi = min(last, R.p0 + SR - 1);
     bool ok;
@@ -441,46 +529,55 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), I.err);
         ok = __syncthreads_and(mine) != 0;
     }
-    const int64_t SZ = nx, SY = (int64_t)nx * nz;
     for (int j = T.ys; j < T.ye && ok; ++j) {
         const int y = j;
         const bool plane_in = j >= EFM_HS && j < ny - EFM_HS;
         const bool rec_plane = (recbits >> (j - T.ys)) & 1ull;
         const bool ypml = j < W || j >= ny - W;
         const float cy_a = ypml ? I.cpml[2 * nx + j] : 0.f, cy_b = ypml ? I.cpml[2 * nx + ny + j] : 0.f;
+        // plane terms of the strip slots
+        const int yr = j - W;
+        const bool yin = yr >= 0 && yr < by;
+        const int yrow = yr < 2 ? yr : (yr >= by - 2 ? 2 + (yr - (by - 2)) : -1);
+        PsiPlane P{nullptr, nullptr, nullptr};
         float pp[ROWS][9];
         if (PASS != EFM_REV) {
+            P = psi_plane(H, j);
 #pragma unroll
             for (int h = 0; h < ROWS; ++h)
-                if (plane_in && colin[h]) load_psi<3>(I, H, x, j, T.z0 + lr + 4 * h, pp[h]);
+                if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
         }
         const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+        const bool store = PASS == EFM_REV || plane_in || rec_plane;
         if (mine && PASS == EFM_REV) {
             // reverse rebuild (-dt, no CPML) into the ping-pong partner f.vo: CPML slabs -> 0,
             // boundary strips -> the values saved at forward step nt-2-it (:1955-1960),
             // box interior -> stencil update, never-updated cells -> 0
             const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
+            const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
 #pragma unroll
             for (int h = 0; h < ROWS; ++h) {
                 if (!colgrid[h]) continue;
-                const int z = T.z0 + lr + 4 * h;
-                const int hi = hidx[h], ci = cidx[h];
-                const int64_t c = x + SZ * z + SY * y;
+                const int hi = rw[h].hidx, ci = rw[h].cidx;
                 float nvx = 0.f, nvy = 0.f, nvz = 0.f;
-                const bool zone = x < W || x >= nx - W || y < W || y >= ny - W || z >= nz - W;
-                int64_t slot[3];
-                const int nslot = zone ? 0 : efm_strip_slots_v(nx, ny, nz, W, x, y, z, slot);
-                if (nslot > 0) {
-                    const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
-                    nvx = sv[slot[0]];
-                    nvy = sv[strip_n + slot[0]];
-                    nvz = sv[2 * strip_n + slot[0]];
-                } else if (!zone && plane_in && colin[h]) {
+                const bool zone = zone_xz[h] || ypml;
+                int slot = -1;
+                if (!zone && yin && sr[h].yf >= 0) {
+                    if (sr[h].xf >= 0) slot = sr[h].xf + yr * bz;
+                    else if (yrow >= 0) slot = sr[h].yf + yrow * bz * bx;
+                    else if (sr[h].zf >= 0) slot = sr[h].zf + yr * bx;
+                }
+                if (slot >= 0) {
+                    nvx = sv[slot];
+                    nvy = sv[strip_n + slot];
+                    nvz = sv[2 * strip_n + slot];
+                } else if (!zone && plane_in && rw[h].in) {
                     const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
                     const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
+                    const float *c0 = R.center(s0, 0) + ci;
                     const float dtxx_dx = t0[hi + 1] - t0[hi];
                     const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
-                    const float dtyy_dy = R.center(sp, 0)[ci] - R.center(s0, 0)[ci];
+                    const float dtyy_dy = R.center(sp, 0)[ci] - c0[0];
                     const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
                     const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
                     const float dtxy_dx = txyc - t3[hi - 1];
@@ -494,33 +591,35 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
                     const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
                     const float k = H.k;
-                    nvx = R.center(s0, 1)[ci] + k * b_x * (dtxx_dx + dtxy_dy + dtxz_dz);
-                    nvy = R.center(s0, 2)[ci] + k * b_y * (dtxy_dx + dtyy_dy + dtyz_dz);
-                    nvz = R.center(s0, 3)[ci] + k * b_z * (dtxz_dx + dtyz_dy + dtzz_dz);
+                    nvx = c0[CF] + k * b_x * (dtxx_dx + dtxy_dy + dtxz_dz);
+                    nvy = c0[2 * CF] + k * b_y * (dtxy_dx + dtyy_dy + dtyz_dz);
+                    nvz = c0[3 * CF] + k * b_z * (dtxz_dx + dtyz_dy + dtzz_dz);
                 }
-                H.out[c] = nvx;
-                H.out[H.nc + c] = nvy;
-                H.out[2 * H.nc + c] = nvz;
+                float *cw = R.center(s0, 1) + ci;
+                cw[0] = nvx;
+                cw[CF] = nvy;
+                cw[2 * CF] = nvz;
             }
+            efm_fence_async_smem();
         } else if (mine) {
             const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
             for (int h = 0; h < ROWS; ++h) {
                 const int z = T.z0 + lr + 4 * h;
-                const bool guard = plane_in && colin[h];
+                const bool guard = plane_in && rw[h].in;
                 const bool rec = rec_plane && colgrid[h] && efm_rec_bit(I, x, y, z);
                 if (!(guard || rec)) continue;
-                const int hi = hidx[h], ci = cidx[h];
-                const int64_t c = x + SZ * z + SY * y;
-                float nvx = R.center(s0, 1)[ci];
-                float nvy = R.center(s0, 2)[ci];
-                float nvz = R.center(s0, 3)[ci];
+                const int hi = rw[h].hidx, ci = rw[h].cidx;
+                float *cw = R.center(s0, 1) + ci;  // vx, vy, vz of this cell
+                float nvx = cw[0];
+                float nvy = cw[CF];
+                float nvz = cw[2 * CF];
                 if (guard) {
                     const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
                     const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
                     const float dtxx_dx = t0[hi + 1] - t0[hi];
                     const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
-                    const float dtyy_dy = R.center(sp, 0)[ci] - R.center(s0, 0)[ci];
+                    const float dtyy_dy = R.center(sp, 0)[ci] - cw[-CF];
                     const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
                     const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
                     const float dtxy_dx = txyc - t3[hi - 1];
@@ -531,41 +630,35 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     const float *p9 = pp[h];
                     float q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f,
                           q8 = 0.f, q9 = 0.f;
-                    if (x < W || x >= nx - W) {
-                        const int xs = x < W ? x : x - (nx - 2 * W);
-                        const int64_t st = (int64_t)ny * nz * 2 * W;
-                        float *p = H.psx + 3 * st + ((int64_t)y * nz + z) * (2 * W) + xs;
+                    if (rw[h].pxo >= 0) {
+                        float *p = P.x + rw[h].pxo;
                         const float a = cx_a, b = cx_b;
                         q1 = b * p9[0] + a * dtxx_dx;
                         q2 = b * p9[1] + a * dtxy_dx;
                         q3 = b * p9[2] + a * dtxz_dx;
                         p[0] = q1;
-                        p[st] = q2;
-                        p[2 * st] = q3;
+                        p[H.stx] = q2;
+                        p[2 * H.stx] = q3;
                     }
-                    if (y < W || y >= ny - W) {
-                        const int ys = y < W ? y : y - (ny - 2 * W);
-                        const int64_t st = (int64_t)2 * W * nz * nx;
-                        float *p = H.psy + 3 * st + ((int64_t)ys * nz + z) * nx + x;
+                    if (P.y != nullptr) {
+                        float *p = P.y + rw[h].pyo;
                         const float a = cy_a, b = cy_b;
                         q4 = b * p9[3] + a * dtyy_dy;
                         q5 = b * p9[4] + a * dtxy_dy;
                         q6 = b * p9[5] + a * dtyz_dy;
                         p[0] = q4;
-                        p[st] = q5;
-                        p[2 * st] = q6;
+                        p[H.sty] = q5;
+                        p[2 * H.sty] = q6;
                     }
-                    if (z >= nz - W) {
-                        const int zs = z - (nz - W);
-                        const int64_t st = (int64_t)ny * W * nx;
-                        float *p = H.psz + 3 * st + ((int64_t)y * W + zs) * nx + x;
+                    if (rw[h].pzo >= 0) {
+                        float *p = P.z + rw[h].pzo;
                         const float a = cz_a[h], b = cz_b[h];
                         q7 = b * p9[6] + a * dtzz_dz;
                         q8 = b * p9[7] + a * dtxz_dz;
                         q9 = b * p9[8] + a * dtyz_dz;
                         p[0] = q7;
-                        p[st] = q8;
-                        p[2 * st] = q9;
+                        p[H.stz] = q8;
+                        p[2 * H.stz] = q9;
                     }
                     // harmonic 2-point buoyancy from the precomputed 1/rho (:153-159)
                     const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];
@@ -581,46 +674,49 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                 if (PASS == EFM_ADJ && rec) {
                     const int tr = I.nt - 1 - it;
                     const int64_t ntr = (int64_t)I.nt * I.nrec;
-                    for (int q = efm_rec_find(I, (int)c); q >= 0 && q < I.nrec && I.rec_lin[q] == (int)c; ++q) {
+                    const int c = x + nx * (z + nz * y);
+                    for (int q = efm_rec_find(I, c); q >= 0 && q < I.nrec && I.rec_lin[q] == c; ++q) {
                         const int64_t o = (int64_t)tr * I.nrec + I.rec_id[q];
                         nvx = __fadd_rn(nvx, I.res[o]);
                         nvy = __fadd_rn(nvy, I.res[ntr + o]);
                         nvz = __fadd_rn(nvz, I.res[2 * ntr + o]);
                     }
                 }
-                H.out[c] = nvx;
-                H.out[H.nc + c] = nvy;
-                H.out[2 * H.nc + c] = nvz;
+                cw[0] = nvx;
+                cw[CF] = nvy;
+                cw[2 * CF] = nvz;
                 if (PASS == EFM_FWD) {
                     if (rec && I.gather != nullptr) {
                         const int64_t ntr = (int64_t)I.nt * I.nrec;
-                        for (int q = efm_rec_find(I, (int)c); q >= 0 && q < I.nrec && I.rec_lin[q] == (int)c; ++q) {
+                        const int c = x + nx * (z + nz * y);
+                        for (int q = efm_rec_find(I, c); q >= 0 && q < I.nrec && I.rec_lin[q] == c; ++q) {
                             const int64_t o = (int64_t)it * I.nrec + I.rec_id[q];
                             I.gather[o] = nvx;
                             I.gather[ntr + o] = nvy;
                             I.gather[2 * ntr + o] = nvz;
                         }
                     }
-                    if (border != nullptr) {
-                        int64_t slot[3];
-                        const int nslot = efm_strip_slots_v(nx, ny, nz, W, x, y, z, slot);
+                    if (border != nullptr && yin && sr[h].yf >= 0) {
                         float *s = border + (int64_t)it * 3 * strip_n;
-                        for (int q = 0; q < nslot; ++q) {
-                            s[slot[q]] = nvx;
-                            s[strip_n + slot[q]] = nvy;
-                            s[2 * strip_n + slot[q]] = nvz;
-                        }
+                        auto put = [&](int sl) {
+                            s[sl] = nvx;
+                            s[strip_n + sl] = nvy;
+                            s[2 * strip_n + sl] = nvz;
+                        };
+                        if (sr[h].xf >= 0) put(sr[h].xf + yr * bz);
+                        if (yrow >= 0) put(sr[h].yf + yrow * bz * bx);
+                        if (sr[h].zf >= 0) put(sr[h].zf + yr * bx);
                     }
                 }
             }
+            if (store) efm_fence_async_smem();
         }
         ok = __syncthreads_and(mine) != 0;
         if (!ok) break;
-        if (j - 1 + SR <= last) {
-            if (threadIdx.x == 0) issue_plane<ROWS, SR, NH, NC>(R, tm, T.x0, T.z0, j - 1 + SR);
-            issued_hi = j - 1 + SR;
-        }
+        if (threadIdx.x == 0) advance<ROWS, SR, NH, NC>(R, tm, stm, 1, 3, store, T.x0, T.z0, j, last);
+        if (j - 1 + SR <= last) issued_hi = j - 1 + SR;
     }
+    if (threadIdx.x == 0) efm_bulk_wait_all();
     if (!ok) drain(R, R.p0, issued_hi);
 }
 

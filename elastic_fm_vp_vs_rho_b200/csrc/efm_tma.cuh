@@ -1,7 +1,7 @@
-// Thin inline-PTX layer for the plane-streaming kernels: mbarriers and TMA tile loads.
+// Thin inline-PTX layer for the plane-streaming kernels: mbarriers, TMA tile loads and stores.
 //
-// Only plain (non-multicast) cp.async.bulk.tensor loads from this GPU's own memory are
-// issued.  Every mbarrier wait is bounded: after EFM_WAIT_LIMIT polls it gives up, sets the
+// Only plain (non-multicast) cp.async.bulk.tensor loads and stores on this GPU's own memory
+// are issued.  Every mbarrier wait is bounded: after EFM_WAIT_LIMIT polls it gives up, sets the
 // context's error word and lets the caller drain and return, so a lost transfer reports an
 // error instead of hanging the GPU.
 #pragma once
@@ -64,6 +64,38 @@ __device__ __forceinline__ void efm_tma_load_3d(void *dst, const CUtensorMap *m,
         " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(efm_smem_addr(dst)),
         "l"(m), "r"(efm_smem_addr(bar)), "r"(x), "r"(z), "r"(y)
         : "memory");
+}
+
+// 3-D tile store from shared memory (x, z, y coordinates), tracked by bulk groups.  The box
+// starts inside the tensor (the callers store whole tiles from non-negative coordinates);
+// elements past the tensor's far edges are not written.
+__device__ __forceinline__ void efm_tma_store_3d(const CUtensorMap *m, const void *src, int x, int z,
+                                                 int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(m),
+        "r"(efm_smem_addr(src)), "r"(x), "r"(z), "r"(y)
+        : "memory");
+}
+
+// Close the current bulk group (an empty one when nothing was issued since the last).
+__device__ __forceinline__ void efm_bulk_commit() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Wait until at most N bulk groups still read their shared-memory source.
+template <int N>
+__device__ __forceinline__ void efm_bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// Wait until every bulk group of this thread has completed (global writes done).
+__device__ __forceinline__ void efm_bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// Order this thread's shared-memory writes before later TMA (async-proxy) reads of them.
+__device__ __forceinline__ void efm_fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // Programmatic dependent launch: let the next kernel in the stream start its prologue now

@@ -306,8 +306,13 @@ bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 
 bool stream_ok(const efm_ctx *ctx) {
     if (!ctx->opt_stream) return false;
-    for (const auto &I : ctx->inst)
+    const int64_t lim = INT32_MAX;
+    for (const auto &I : ctx->inst) {
         if (I.nx % 4 != 0 || !aligned16(I.lam) || !aligned16(I.mu) || !aligned16(I.rho)) return false;
+        // the streaming kernels address memory variables, strips and cells with 32-bit offsets
+        if (6 * std::max({I.psx_n, I.psy_n, I.psz_n}) > lim || 3 * I.strip_n > lim || I.ncell > lim)
+            return false;
+    }
     return true;
 }
 

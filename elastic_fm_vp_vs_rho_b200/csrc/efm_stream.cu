@@ -160,11 +160,13 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
 // Per-block constants of the plane loop, read from the instance table once.  The loop's
 // mbarrier waits are asm statements with a memory clobber, after which the compiler would
 // otherwise reload every table field it touches.  The memory variables of a pass are three
-// consecutive components of each slab family (FIRST 0: stress, 3: velocity).
+// consecutive components of each slab family (FIRST 0: stress, 3: velocity); every offset
+// into a family fits 32 bits (the host checks), so addresses are one 32-bit add and one
+// wide multiply-add off a 64-bit base instead of 64-bit index arithmetic.
 struct Hot {
     float *psx, *psy, *psz;  // component FIRST of each family
-    int64_t stx, sty, stz;   // component strides
-    int64_t pxs, pys, pzs;   // plane strides: nz*2W (x slabs), nz*nx (y slabs), W*nx (z slab)
+    int stx, sty, stz;       // component strides
+    int pxs, pys, pzs;       // plane strides: nz*2W (x slabs), nz*nx (y slabs), W*nx (z slab)
     float k;
     int nx, ny, nz, W;
 };
@@ -175,15 +177,15 @@ __device__ __forceinline__ Hot make_hot(const EfmInst &I, int first) {
     h.ny = I.ny;
     h.nz = I.nz;
     h.W = I.W;
-    h.stx = (int64_t)I.ny * I.nz * 2 * I.W;
-    h.sty = (int64_t)2 * I.W * I.nz * I.nx;
-    h.stz = (int64_t)I.ny * I.W * I.nx;
-    h.pxs = (int64_t)I.nz * 2 * I.W;
-    h.pys = (int64_t)I.nz * I.nx;
-    h.pzs = (int64_t)I.W * I.nx;
-    h.psx = I.psi_x + first * h.stx;
-    h.psy = I.psi_y + first * h.sty;
-    h.psz = I.psi_z + first * h.stz;
+    h.stx = I.ny * I.nz * 2 * I.W;
+    h.sty = 2 * I.W * I.nz * I.nx;
+    h.stz = I.ny * I.W * I.nx;
+    h.pxs = I.nz * 2 * I.W;
+    h.pys = I.nz * I.nx;
+    h.pzs = I.W * I.nx;
+    h.psx = I.psi_x + (int64_t)first * h.stx;
+    h.psy = I.psi_y + (int64_t)first * h.sty;
+    h.psz = I.psi_z + (int64_t)first * h.stz;
     h.k = I.k;
     return h;
 }
@@ -194,42 +196,43 @@ struct Row {
     int hidx, cidx;
     int pxo, pyo, pzo;
     bool in;
+    bool wx, wz;  // some lane of this warp has an x (z) memory variable in this row
 };
 
-// Memory-variable rows of one plane (component FIRST; y null outside the y slabs).
+// Plane offsets of the three families (y: only on the planes of the y slabs).
 struct PsiPlane {
-    float *x, *y, *z;
+    int x, y, z;
+    bool has_y;
 };
 
 __device__ __forceinline__ PsiPlane psi_plane(const Hot &H, int y) {
     PsiPlane P;
-    P.x = H.psx + (int64_t)y * H.pxs;
-    P.z = H.psz + (int64_t)y * H.pzs;
-    P.y = nullptr;
-    if (y < H.W) P.y = H.psy + (int64_t)y * H.pys;
-    else if (y >= H.ny - H.W) P.y = H.psy + (int64_t)(y - (H.ny - 2 * H.W)) * H.pys;
+    P.x = y * H.pxs;
+    P.z = y * H.pzs;
+    P.has_y = y < H.W || y >= H.ny - H.W;
+    P.y = (y < H.W ? y : y - (H.ny - 2 * H.W)) * H.pys;
     return P;
 }
 
-// Request the 9 old memory variables of one cell (zeros where it has none): 0-2 x family,
-// 3-5 y family, 6-8 z family.
+// Request the old memory variables of one cell that it has (0-2 x family, 3-5 y family, 6-8
+// z family; the others are left unset and never read).  Each family sits behind a test that
+// is uniform over the warp (the row flags) or the block (the plane), so warps without memory
+// variables of a family branch past its code.
 __device__ __forceinline__ void load_psi(const Hot &H, const PsiPlane &P, const Row &r, float *pp) {
-#pragma unroll
-    for (int q = 0; q < 9; ++q) pp[q] = 0.f;
-    if (r.pxo >= 0) {
-        const float *p = P.x + r.pxo;
+    if (r.wx && r.pxo >= 0) {
+        const float *p = H.psx + (P.x + r.pxo);
         pp[0] = p[0];
         pp[1] = p[H.stx];
         pp[2] = p[2 * H.stx];
     }
-    if (P.y != nullptr) {
-        const float *p = P.y + r.pyo;
+    if (P.has_y) {
+        const float *p = H.psy + (P.y + r.pyo);
         pp[3] = p[0];
         pp[4] = p[H.sty];
         pp[5] = p[2 * H.sty];
     }
-    if (r.pzo >= 0) {
-        const float *p = P.z + r.pzo;
+    if (r.wz && r.pzo >= 0) {
+        const float *p = H.psz + (P.z + r.pzo);
         pp[6] = p[0];
         pp[7] = p[H.stz];
         pp[8] = p[2 * H.stz];
@@ -267,8 +270,8 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
     float pvz_z = 0.f, pvx_z = 0.f, pvy_z = 0.f;
     if (PASS != EFM_REV) {
         // pp: the 9 old memory variables requested at the top of the iteration
-        if (rw.pxo >= 0) {
-            float *p = P.x + rw.pxo;
+        if (rw.wx && rw.pxo >= 0) {
+            float *p = H.psx + (P.x + rw.pxo);
             const float a = C.ax, b = C.bx;
             pvx_x = b * pp[0] + a * dvx_dx;
             pvy_x = b * pp[1] + a * dvy_dx;
@@ -277,8 +280,8 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
             p[H.stx] = pvy_x;
             p[2 * H.stx] = pvz_x;
         }
-        if (P.y != nullptr) {
-            float *p = P.y + rw.pyo;
+        if (P.has_y) {
+            float *p = H.psy + (P.y + rw.pyo);
             const float a = C.ay, b = C.by;
             pvy_y = b * pp[3] + a * dvy_dy;
             pvx_y = b * pp[4] + a * dvx_dy;
@@ -287,8 +290,8 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
             p[H.sty] = pvx_y;
             p[2 * H.sty] = pvz_y;
         }
-        if (rw.pzo >= 0) {
-            float *p = P.z + rw.pzo;
+        if (rw.wz && rw.pzo >= 0) {
+            float *p = H.psz + (P.z + rw.pzo);
             const float a = C.az, b = C.bz;
             pvz_z = b * pp[6] + a * dvz_dz;
             pvx_z = b * pp[7] + a * dvx_dz;
@@ -372,6 +375,8 @@ __device__ __forceinline__ void make_rows(const Hot &H, const Tile &T, int x, in
         rw[h].pxo = xpml && z < nz ? z * 2 * W + xs : -1;
         rw[h].pyo = z * nx + x;
         rw[h].pzo = z < nz && z >= nz - W && x < nx ? (z - (nz - W)) * nx + x : -1;
+        rw[h].wx = __any_sync(0xffffffffu, rw[h].pxo >= 0);
+        rw[h].wz = __any_sync(0xffffffffu, rw[h].pzo >= 0);
     }
 }
 
@@ -450,7 +455,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
             cf[h].ay = cy_a;
             cf[h].by = cy_b;
         }
-        PsiPlane P{nullptr, nullptr, nullptr};
+        PsiPlane P{0, 0, 0, false};
         float pp[ROWS][9];
         if (PASS != EFM_REV) {
             P = psi_plane(H, j);
@@ -539,7 +544,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
         const int yr = j - W;
         const bool yin = yr >= 0 && yr < by;
         const int yrow = yr < 2 ? yr : (yr >= by - 2 ? 2 + (yr - (by - 2)) : -1);
-        PsiPlane P{nullptr, nullptr, nullptr};
+        PsiPlane P{0, 0, 0, false};
         float pp[ROWS][9];
         if (PASS != EFM_REV) {
             P = psi_plane(H, j);
@@ -630,8 +635,8 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     const float *p9 = pp[h];
                     float q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f,
                           q8 = 0.f, q9 = 0.f;
-                    if (rw[h].pxo >= 0) {
-                        float *p = P.x + rw[h].pxo;
+                    if (rw[h].wx && rw[h].pxo >= 0) {
+                        float *p = H.psx + (P.x + rw[h].pxo);
                         const float a = cx_a, b = cx_b;
                         q1 = b * p9[0] + a * dtxx_dx;
                         q2 = b * p9[1] + a * dtxy_dx;
@@ -640,8 +645,8 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                         p[H.stx] = q2;
                         p[2 * H.stx] = q3;
                     }
-                    if (P.y != nullptr) {
-                        float *p = P.y + rw[h].pyo;
+                    if (P.has_y) {
+                        float *p = H.psy + (P.y + rw[h].pyo);
                         const float a = cy_a, b = cy_b;
                         q4 = b * p9[3] + a * dtyy_dy;
                         q5 = b * p9[4] + a * dtxy_dy;
@@ -650,8 +655,8 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                         p[H.sty] = q5;
                         p[2 * H.sty] = q6;
                     }
-                    if (rw[h].pzo >= 0) {
-                        float *p = P.z + rw[h].pzo;
+                    if (rw[h].wz && rw[h].pzo >= 0) {
+                        float *p = H.psz + (P.z + rw[h].pzo);
                         const float a = cz_a[h], b = cz_b[h];
                         q7 = b * p9[6] + a * dtzz_dz;
                         q8 = b * p9[7] + a * dtxz_dz;

@@ -310,7 +310,7 @@ bool stream_ok(const efm_ctx *ctx) {
     for (const auto &I : ctx->inst) {
         if (I.nx % 4 != 0 || !aligned16(I.lam) || !aligned16(I.mu) || !aligned16(I.rho)) return false;
         // the streaming kernels address memory variables, strips and cells with 32-bit offsets
-        if (6 * std::max({I.psx_n, I.psy_n, I.psz_n}) > lim || 3 * I.strip_n > lim || I.ncell > lim)
+        if (8 * std::max({I.psx_n, I.psy_n, I.psz_n}) > lim || 3 * I.strip_n > lim || I.ncell > lim)
             return false;
     }
     return true;
@@ -480,7 +480,7 @@ int ensure_workspace(efm_ctx *ctx, bool grad, bool borders) {
             }
         }
         if (I.psi == nullptr) {
-            const size_t np = 6 * (size_t)(I.psx_n + I.psy_n + I.psz_n);
+            const size_t np = EFM_PSI_PER_CELL * (size_t)(I.psx_n + I.psy_n + I.psz_n);
             if (cudaMalloc(&I.psi, np * sizeof(float)) != cudaSuccess) {
                 cudaGetLastError();
                 return fail(EFM_ERR_NOMEM, "cannot allocate CPML memory variables");
@@ -518,8 +518,8 @@ EfmInst base_table(const Inst &I) {
     d.rho = I.rho;
     d.cpml = I.cpml;
     d.psi_x = I.psi;
-    d.psi_y = I.psi + 6 * I.psx_n;
-    d.psi_z = I.psi + 6 * (I.psx_n + I.psy_n);
+    d.psi_y = I.psi + EFM_PSI_PER_CELL * I.psx_n;
+    d.psi_z = I.psi + EFM_PSI_PER_CELL * (I.psx_n + I.psy_n);
     d.nsrc = I.nsrc;
     for (int s = 0; s < EFM_NSRC; ++s) {
         d.sx[s] = I.src[s][0];
@@ -540,8 +540,10 @@ EfmInst base_table(const Inst &I) {
     return d;
 }
 
+size_t psi_floats(const Inst &I) { return EFM_PSI_PER_CELL * (size_t)(I.psx_n + I.psy_n + I.psz_n); }
+
 int zero_psi(const Inst &I, cudaStream_t s) {
-    EFM_CK(cudaMemsetAsync(I.psi, 0, 6 * (size_t)(I.psx_n + I.psy_n + I.psz_n) * sizeof(float), s));
+    EFM_CK(cudaMemsetAsync(I.psi, 0, psi_floats(I) * sizeof(float), s));
     return EFM_OK;
 }
 
@@ -557,7 +559,6 @@ int check_ready(efm_ctx *ctx) {
 }
 
 
-size_t psi_floats(const Inst &I) { return 6 * (size_t)(I.psx_n + I.psy_n + I.psz_n); }
 size_t ckpt_floats(const Inst &I) { return 9 * (size_t)I.ncell + psi_floats(I); }
 
 // Workspace of the exact adjoint (checkpoint interval from the context option).
@@ -1040,7 +1041,7 @@ int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders) {
     int64_t b = 0;
     for (const Inst &I : ctx->inst) {
         b += (save_borders ? 23 : 11) * I.ncell * 4;
-        b += 6 * (I.psx_n + I.psy_n + I.psz_n) * 4;
+        b += EFM_PSI_PER_CELL * (I.psx_n + I.psy_n + I.psz_n) * 4;
         if (save_borders) b += (int64_t)I.nt * 3 * I.strip_n * 4;
     }
     return b;

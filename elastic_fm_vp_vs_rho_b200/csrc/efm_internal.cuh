@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#define EFM_PSI_PER_CELL 8  // floats of CPML memory variables per cell of a slab family
 #define EFM_HS 2            // interior guard H_STENCIL (mainPropElastic3D_MT.py:54)
 #define EFM_TX 32          // tile: one warp along x ...
 #define EFM_TZ 4           // ... 4 rows along z ...
@@ -42,11 +43,13 @@ struct EfmInst {
     const float *lam, *mu, *rho;
     const float *cpml; // ax[nx] bx[nx] ay[ny] by[ny] az[nz] bz[nz]
     EfmFields f;
-    // compact CPML memory variables; 6 per slab family: 3 read by the stress update
-    // (d/dx of vx, vy, vz ...) followed by 3 read by the velocity update
-    float *psi_x;      // [6][ny][nz][2W]
-    float *psi_y;      // [6][2W][nz][nx]
-    float *psi_z;      // [6][ny][W][nx]   (bottom face only; the top has no CPML)
+    // compact CPML memory variables; per slab family two groups of the family's cells, the
+    // stress update's three (of d/dx vx, vy, vz ...) then the velocity update's three, each
+    // cell's three components packed with a pad into one 16-byte vector (EFM_PSI_PER_CELL
+    // floats per cell of a family)
+    float *psi_x;      // [2][ny][nz][2W][4]
+    float *psi_y;      // [2][2W][nz][nx][4]
+    float *psi_z;      // [2][ny][W][nx][4]   (bottom face only; the top has no CPML)
     int nsrc;
     int sx[EFM_NSRC], sy[EFM_NSRC], sz[EFM_NSRC];
     float mt[EFM_NSRC][6];

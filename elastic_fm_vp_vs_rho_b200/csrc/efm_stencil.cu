@@ -20,10 +20,14 @@ namespace {
 __device__ __forceinline__ float rcp(float a) { return __frcp_rn(a); }
 
 // psi = b psi + a d on one slab entry; returns the new psi.
-__device__ __forceinline__ float psi_upd(float *p, float a, float b, float d) {
-    float v = b * (*p) + a * d;
-    *p = v;
-    return v;
+// psi <- b psi + a d for the three packed components of one cell (one 16-byte load and store)
+__device__ __forceinline__ void psi_upd(float4 *p, float a, float b, float d0, float d1, float d2,
+                                        float &v0, float &v1, float &v2) {
+    const float4 o = *p;
+    v0 = b * o.x + a * d0;
+    v1 = b * o.y + a * d1;
+    v2 = b * o.z + a * d2;
+    *p = make_float4(v0, v1, v2, 0.f);
 }
 
 }  // namespace
@@ -65,30 +69,21 @@ efm_stress_kernel(const EfmInst *__restrict__ insts, int ninst, int it) {
     if (PASS != EFM_REV) {
         if (x < W || x >= nx - W) {
             const int xs = x < W ? x : x - (nx - 2 * W);
-            const int64_t st = (int64_t)ny * nz * 2 * W;
-            float *p = I.psi_x + ((int64_t)y * nz + z) * (2 * W) + xs;
+            float4 *p = reinterpret_cast<float4 *>(I.psi_x) + ((int64_t)y * nz + z) * (2 * W) + xs;
             const float a = I.cpml[x], b = I.cpml[nx + x];
-            pvx_x = psi_upd(p, a, b, dvx_dx);
-            pvy_x = psi_upd(p + st, a, b, dvy_dx);
-            pvz_x = psi_upd(p + 2 * st, a, b, dvz_dx);
+            psi_upd(p, a, b, dvx_dx, dvy_dx, dvz_dx, pvx_x, pvy_x, pvz_x);
         }
         if (y < W || y >= ny - W) {
             const int ys = y < W ? y : y - (ny - 2 * W);
-            const int64_t st = (int64_t)2 * W * nz * nx;
-            float *p = I.psi_y + ((int64_t)ys * nz + z) * nx + x;
+            float4 *p = reinterpret_cast<float4 *>(I.psi_y) + ((int64_t)ys * nz + z) * nx + x;
             const float a = I.cpml[2 * nx + y], b = I.cpml[2 * nx + ny + y];
-            pvy_y = psi_upd(p, a, b, dvy_dy);
-            pvx_y = psi_upd(p + st, a, b, dvx_dy);
-            pvz_y = psi_upd(p + 2 * st, a, b, dvz_dy);
+            psi_upd(p, a, b, dvy_dy, dvx_dy, dvz_dy, pvy_y, pvx_y, pvz_y);
         }
         if (z >= nz - W) {
             const int zs = z - (nz - W);
-            const int64_t st = (int64_t)ny * W * nx;
-            float *p = I.psi_z + ((int64_t)y * W + zs) * nx + x;
+            float4 *p = reinterpret_cast<float4 *>(I.psi_z) + ((int64_t)y * W + zs) * nx + x;
             const float a = I.cpml[2 * nx + 2 * ny + z], b = I.cpml[2 * nx + 2 * ny + nz + z];
-            pvz_z = psi_upd(p, a, b, dvz_dz);
-            pvx_z = psi_upd(p + st, a, b, dvx_dz);
-            pvy_z = psi_upd(p + 2 * st, a, b, dvy_dz);
+            psi_upd(p, a, b, dvz_dz, dvx_dz, dvy_dz, pvz_z, pvx_z, pvy_z);
         }
     }
 
@@ -216,32 +211,27 @@ efm_velocity_kernel(const EfmInst *__restrict__ insts, int ninst, int it) {
         float p1 = 0.f, p2 = 0.f, p3 = 0.f, p4 = 0.f, p5 = 0.f, p6 = 0.f, p7 = 0.f, p8 = 0.f,
               p9 = 0.f;
         if (PASS != EFM_REV) {
+            // second group of each family: the velocity update's memory variables
             if (x < W || x >= nx - W) {
                 const int xs = x < W ? x : x - (nx - 2 * W);
-                const int64_t st = (int64_t)ny * nz * 2 * W;
-                float *p = I.psi_x + 3 * st + ((int64_t)y * nz + z) * (2 * W) + xs;
+                const int64_t n = (int64_t)ny * nz * 2 * W;
+                float4 *p = reinterpret_cast<float4 *>(I.psi_x) + n + ((int64_t)y * nz + z) * (2 * W) + xs;
                 const float a = I.cpml[x], b = I.cpml[nx + x];
-                p1 = psi_upd(p, a, b, dtxx_dx);
-                p2 = psi_upd(p + st, a, b, dtxy_dx);
-                p3 = psi_upd(p + 2 * st, a, b, dtxz_dx);
+                psi_upd(p, a, b, dtxx_dx, dtxy_dx, dtxz_dx, p1, p2, p3);
             }
             if (y < W || y >= ny - W) {
                 const int ys = y < W ? y : y - (ny - 2 * W);
-                const int64_t st = (int64_t)2 * W * nz * nx;
-                float *p = I.psi_y + 3 * st + ((int64_t)ys * nz + z) * nx + x;
+                const int64_t n = (int64_t)2 * W * nz * nx;
+                float4 *p = reinterpret_cast<float4 *>(I.psi_y) + n + ((int64_t)ys * nz + z) * nx + x;
                 const float a = I.cpml[2 * nx + y], b = I.cpml[2 * nx + ny + y];
-                p4 = psi_upd(p, a, b, dtyy_dy);
-                p5 = psi_upd(p + st, a, b, dtxy_dy);
-                p6 = psi_upd(p + 2 * st, a, b, dtyz_dy);
+                psi_upd(p, a, b, dtyy_dy, dtxy_dy, dtyz_dy, p4, p5, p6);
             }
             if (z >= nz - W) {
                 const int zs = z - (nz - W);
-                const int64_t st = (int64_t)ny * W * nx;
-                float *p = I.psi_z + 3 * st + ((int64_t)y * W + zs) * nx + x;
+                const int64_t n = (int64_t)ny * W * nx;
+                float4 *p = reinterpret_cast<float4 *>(I.psi_z) + n + ((int64_t)y * W + zs) * nx + x;
                 const float a = I.cpml[2 * nx + 2 * ny + z], b = I.cpml[2 * nx + 2 * ny + nz + z];
-                p7 = psi_upd(p, a, b, dtzz_dz);
-                p8 = psi_upd(p + st, a, b, dtxz_dz);
-                p9 = psi_upd(p + 2 * st, a, b, dtyz_dz);
+                psi_upd(p, a, b, dtzz_dz, dtxz_dz, dtyz_dz, p7, p8, p9);
             }
         }
         // harmonic 2-point buoyancy at the velocity points (:153-159)

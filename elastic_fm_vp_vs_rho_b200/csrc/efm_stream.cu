@@ -159,33 +159,29 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
 
 // Per-block constants of the plane loop, read from the instance table once.  The loop's
 // mbarrier waits are asm statements with a memory clobber, after which the compiler would
-// otherwise reload every table field it touches.  The memory variables of a pass are three
-// consecutive components of each slab family (FIRST 0: stress, 3: velocity); every offset
-// into a family fits 32 bits (the host checks), so addresses are one 32-bit add and one
-// wide multiply-add off a 64-bit base instead of 64-bit index arithmetic.
+// otherwise reload every table field it touches.  The memory variables of a pass are one
+// group of each slab family (0: stress, 1: velocity), a 16-byte vector per cell; every cell
+// offset into a family fits 32 bits (the host checks), so an address is one 32-bit add and
+// one wide multiply-add off a 64-bit base.
 struct Hot {
-    float *psx, *psy, *psz;  // component FIRST of each family
-    int stx, sty, stz;       // component strides
-    int pxs, pys, pzs;       // plane strides: nz*2W (x slabs), nz*nx (y slabs), W*nx (z slab)
+    float4 *psx, *psy, *psz;  // this pass's group of each family
+    int pxs, pys, pzs;        // plane strides in cells: nz*2W (x slabs), nz*nx (y slabs), W*nx (z)
     float k;
     int nx, ny, nz, W;
 };
 
-__device__ __forceinline__ Hot make_hot(const EfmInst &I, int first) {
+__device__ __forceinline__ Hot make_hot(const EfmInst &I, int group) {
     Hot h;
     h.nx = I.nx;
     h.ny = I.ny;
     h.nz = I.nz;
     h.W = I.W;
-    h.stx = I.ny * I.nz * 2 * I.W;
-    h.sty = 2 * I.W * I.nz * I.nx;
-    h.stz = I.ny * I.W * I.nx;
     h.pxs = I.nz * 2 * I.W;
     h.pys = I.nz * I.nx;
     h.pzs = I.W * I.nx;
-    h.psx = I.psi_x + (int64_t)first * h.stx;
-    h.psy = I.psi_y + (int64_t)first * h.sty;
-    h.psz = I.psi_z + (int64_t)first * h.stz;
+    h.psx = reinterpret_cast<float4 *>(I.psi_x) + (int64_t)group * I.ny * h.pxs;
+    h.psy = reinterpret_cast<float4 *>(I.psi_y) + (int64_t)group * 2 * I.W * h.pys;
+    h.psz = reinterpret_cast<float4 *>(I.psi_z) + (int64_t)group * I.ny * h.pzs;
     h.k = I.k;
     return h;
 }
@@ -220,22 +216,22 @@ __device__ __forceinline__ PsiPlane psi_plane(const Hot &H, int y) {
 // variables of a family branch past its code.
 __device__ __forceinline__ void load_psi(const Hot &H, const PsiPlane &P, const Row &r, float *pp) {
     if (r.wx && r.pxo >= 0) {
-        const float *p = H.psx + (P.x + r.pxo);
-        pp[0] = p[0];
-        pp[1] = p[H.stx];
-        pp[2] = p[2 * H.stx];
+        const float4 v = H.psx[P.x + r.pxo];
+        pp[0] = v.x;
+        pp[1] = v.y;
+        pp[2] = v.z;
     }
     if (P.has_y) {
-        const float *p = H.psy + (P.y + r.pyo);
-        pp[3] = p[0];
-        pp[4] = p[H.sty];
-        pp[5] = p[2 * H.sty];
+        const float4 v = H.psy[P.y + r.pyo];
+        pp[3] = v.x;
+        pp[4] = v.y;
+        pp[5] = v.z;
     }
     if (r.wz && r.pzo >= 0) {
-        const float *p = H.psz + (P.z + r.pzo);
-        pp[6] = p[0];
-        pp[7] = p[H.stz];
-        pp[8] = p[2 * H.stz];
+        const float4 v = H.psz[P.z + r.pzo];
+        pp[6] = v.x;
+        pp[7] = v.y;
+        pp[8] = v.z;
     }
 }
 
@@ -271,34 +267,25 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
     if (PASS != EFM_REV) {
         // pp: the 9 old memory variables requested at the top of the iteration
         if (rw.wx && rw.pxo >= 0) {
-            float *p = H.psx + (P.x + rw.pxo);
             const float a = C.ax, b = C.bx;
             pvx_x = b * pp[0] + a * dvx_dx;
             pvy_x = b * pp[1] + a * dvy_dx;
             pvz_x = b * pp[2] + a * dvz_dx;
-            p[0] = pvx_x;
-            p[H.stx] = pvy_x;
-            p[2 * H.stx] = pvz_x;
+            H.psx[P.x + rw.pxo] = make_float4(pvx_x, pvy_x, pvz_x, 0.f);
         }
         if (P.has_y) {
-            float *p = H.psy + (P.y + rw.pyo);
             const float a = C.ay, b = C.by;
             pvy_y = b * pp[3] + a * dvy_dy;
             pvx_y = b * pp[4] + a * dvx_dy;
             pvz_y = b * pp[5] + a * dvz_dy;
-            p[0] = pvy_y;
-            p[H.sty] = pvx_y;
-            p[2 * H.sty] = pvz_y;
+            H.psy[P.y + rw.pyo] = make_float4(pvy_y, pvx_y, pvz_y, 0.f);
         }
         if (rw.wz && rw.pzo >= 0) {
-            float *p = H.psz + (P.z + rw.pzo);
             const float a = C.az, b = C.bz;
             pvz_z = b * pp[6] + a * dvz_dz;
             pvx_z = b * pp[7] + a * dvx_dz;
             pvy_z = b * pp[8] + a * dvy_dz;
-            p[0] = pvz_z;
-            p[H.stz] = pvx_z;
-            p[2 * H.stz] = pvy_z;
+            H.psz[P.z + rw.pzo] = make_float4(pvz_z, pvx_z, pvy_z, 0.f);
         }
     }
     // harmonic 4-point averages of mu from the precomputed 1/mu (:80-89)
@@ -504,7 +491,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
     const unsigned long long recbits = s_rec;
-    const Hot H = make_hot(I, 3);
+    const Hot H = make_hot(I, 1);
     float *const border = I.border;
     const int64_t strip_n = I.strip_n;
     const int by = ny - 2 * W, bx = nx - 2 * W, bz = nz - W - 2;
@@ -636,34 +623,25 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     float q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f,
                           q8 = 0.f, q9 = 0.f;
                     if (rw[h].wx && rw[h].pxo >= 0) {
-                        float *p = H.psx + (P.x + rw[h].pxo);
                         const float a = cx_a, b = cx_b;
                         q1 = b * p9[0] + a * dtxx_dx;
                         q2 = b * p9[1] + a * dtxy_dx;
                         q3 = b * p9[2] + a * dtxz_dx;
-                        p[0] = q1;
-                        p[H.stx] = q2;
-                        p[2 * H.stx] = q3;
+                        H.psx[P.x + rw[h].pxo] = make_float4(q1, q2, q3, 0.f);
                     }
                     if (P.has_y) {
-                        float *p = H.psy + (P.y + rw[h].pyo);
                         const float a = cy_a, b = cy_b;
                         q4 = b * p9[3] + a * dtyy_dy;
                         q5 = b * p9[4] + a * dtxy_dy;
                         q6 = b * p9[5] + a * dtyz_dy;
-                        p[0] = q4;
-                        p[H.sty] = q5;
-                        p[2 * H.sty] = q6;
+                        H.psy[P.y + rw[h].pyo] = make_float4(q4, q5, q6, 0.f);
                     }
                     if (rw[h].wz && rw[h].pzo >= 0) {
-                        float *p = H.psz + (P.z + rw[h].pzo);
                         const float a = cz_a[h], b = cz_b[h];
                         q7 = b * p9[6] + a * dtzz_dz;
                         q8 = b * p9[7] + a * dtxz_dz;
                         q9 = b * p9[8] + a * dtyz_dz;
-                        p[0] = q7;
-                        p[H.stz] = q8;
-                        p[2 * H.stz] = q9;
+                        H.psz[P.z + rw[h].pzo] = make_float4(q7, q8, q9, 0.f);
                     }
                     // harmonic 2-point buoyancy from the precomputed 1/rho (:153-159)
                     const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];

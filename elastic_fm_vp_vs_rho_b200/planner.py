@@ -18,7 +18,7 @@ import math
 def _geometry(nx, ny, nz, lenpml):
     W = lenpml
     ncell = nx * ny * nz
-    psi = 6 * (ny * nz * 2 * W + 2 * W * nz * nx + ny * W * nx)
+    psi = 8 * (ny * nz * 2 * W + 2 * W * nz * nx + ny * W * nx)  # two packed groups per slab cell
     bx, by, bz = nx - 2 * W, ny - 2 * W, nz - W - 2
     strip = 4 * by * bz + 4 * bz * bx + 4 * by * bx
     return ncell, psi, strip

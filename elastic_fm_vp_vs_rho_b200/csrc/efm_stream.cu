@@ -36,6 +36,13 @@ __device__ __forceinline__ float frcp(float a) {
     return r;
 }
 
+// Compile-time flag for the two instantiations of a plane's update (with / without the CPML
+// memory-variable code); a warp picks one per plane with a warp-uniform test.
+template <bool B>
+struct Tag {
+    static constexpr bool value = B;
+};
+
 template <int ROWS, int SR>
 struct Ring {
     static constexpr int HB = efm_halo_bytes(ROWS), CB = efm_center_bytes(ROWS);
@@ -243,7 +250,7 @@ struct Coef {
 
 // New stress of one cell, written over its old stress in the ring (the block stores the
 // plane with TMA afterwards).
-template <int PASS, int ROWS, int SR>
+template <int PASS, int ROWS, int SR, bool PML>
 __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, SR> &R, int sm, int s0,
                                             int sp, int it, int x, int y, int z, const Row &rw,
                                             bool has_src, const float *pp, const Coef &C,
@@ -264,8 +271,8 @@ __device__ __forceinline__ void stress_cell(const EfmInst &I, const Ring<ROWS, S
     const float dvz_dy = R.halo(sp, 2)[hidx] - vzc;
     float pvx_x = 0.f, pvy_x = 0.f, pvz_x = 0.f, pvy_y = 0.f, pvx_y = 0.f, pvz_y = 0.f;
     float pvz_z = 0.f, pvx_z = 0.f, pvy_z = 0.f;
-    if (PASS != EFM_REV) {
-        // pp: the 9 old memory variables requested at the top of the iteration
+    if (PML && PASS != EFM_REV) {
+        // pp: the old memory variables requested at the top of the iteration
         if (rw.wx && rw.pxo >= 0) {
             const float a = C.ax, b = C.bx;
             pvx_x = b * pp[0] + a * dvx_dx;
@@ -442,24 +449,36 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
             cf[h].ay = cy_a;
             cf[h].by = cy_b;
         }
-        PsiPlane P{0, 0, 0, false};
-        float pp[ROWS][9];
+        // the plane's update, with or without the memory-variable code
+        auto plane = [&](auto tag) -> bool {
+            constexpr bool PML = decltype(tag)::value;
+            PsiPlane P{0, 0, 0, false};
+            float pp[ROWS][9];
+            if (PML) {
+                P = psi_plane(H, j);
+#pragma unroll
+                for (int h = 0; h < ROWS; ++h)
+                    if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
+            }
+            const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+            if (mine && plane_in) {
+                const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
+#pragma unroll
+                for (int h = 0; h < ROWS; ++h)
+                    if (rw[h].in)
+                        stress_cell<PASS, ROWS, SR, PML>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h,
+                                                         rw[h], has_src, pp[h], cf[h], H, P);
+                efm_fence_async_smem();
+            }
+            return mine;
+        };
+        bool wpml = false;  // warp-uniform: some lane of this warp has memory variables here
         if (PASS != EFM_REV) {
-            P = psi_plane(H, j);
+            wpml = ypml;
 #pragma unroll
-            for (int h = 0; h < ROWS; ++h)
-                if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
+            for (int h = 0; h < ROWS; ++h) wpml = wpml || rw[h].wx || rw[h].wz;
         }
-        const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
-        if (mine && plane_in) {
-            const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
-#pragma unroll
-            for (int h = 0; h < ROWS; ++h)
-                if (rw[h].in)
-                    stress_cell<PASS, ROWS, SR>(I, R, sm, s0, sp, it, x, j, T.z0 + lr + 4 * h, rw[h],
-                                                has_src, pp[h], cf[h], H, P);
-            efm_fence_async_smem();
-        }
+        const bool mine = wpml ? plane(Tag<true>{}) : plane(Tag<false>{});
         ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
         if (!ok) break;
         if (threadIdx.x == 0)
@@ -531,168 +550,182 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
         const int yr = j - W;
         const bool yin = yr >= 0 && yr < by;
         const int yrow = yr < 2 ? yr : (yr >= by - 2 ? 2 + (yr - (by - 2)) : -1);
-        PsiPlane P{0, 0, 0, false};
-        float pp[ROWS][9];
-        if (PASS != EFM_REV) {
-            P = psi_plane(H, j);
-#pragma unroll
-            for (int h = 0; h < ROWS; ++h)
-                if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
-        }
-        const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
         const bool store = PASS == EFM_REV || plane_in || rec_plane;
-        if (mine && PASS == EFM_REV) {
-            // reverse rebuild (-dt, no CPML) into the ping-pong partner f.vo: CPML slabs -> 0,
-            // boundary strips -> the values saved at forward step nt-2-it (:1955-1960),
-            // box interior -> stencil update, never-updated cells -> 0
-            const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
-            const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
+        bool mine;
+        if (PASS == EFM_REV) {
+            mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+            if (mine) {
+                // reverse rebuild (-dt, no CPML) into the ping-pong partner f.vo: CPML slabs -> 0,
+                // boundary strips -> the values saved at forward step nt-2-it (:1955-1960),
+                // box interior -> stencil update, never-updated cells -> 0
+                const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
+                const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
 #pragma unroll
-            for (int h = 0; h < ROWS; ++h) {
-                if (!colgrid[h]) continue;
-                const int hi = rw[h].hidx, ci = rw[h].cidx;
-                float nvx = 0.f, nvy = 0.f, nvz = 0.f;
-                const bool zone = zone_xz[h] || ypml;
-                int slot = -1;
-                if (!zone && yin && sr[h].yf >= 0) {
-                    if (sr[h].xf >= 0) slot = sr[h].xf + yr * bz;
-                    else if (yrow >= 0) slot = sr[h].yf + yrow * bz * bx;
-                    else if (sr[h].zf >= 0) slot = sr[h].zf + yr * bx;
+                for (int h = 0; h < ROWS; ++h) {
+                    if (!colgrid[h]) continue;
+                    const int hi = rw[h].hidx, ci = rw[h].cidx;
+                    float nvx = 0.f, nvy = 0.f, nvz = 0.f;
+                    const bool zone = zone_xz[h] || ypml;
+                    int slot = -1;
+                    if (!zone && yin && sr[h].yf >= 0) {
+                        if (sr[h].xf >= 0) slot = sr[h].xf + yr * bz;
+                        else if (yrow >= 0) slot = sr[h].yf + yrow * bz * bx;
+                        else if (sr[h].zf >= 0) slot = sr[h].zf + yr * bx;
+                    }
+                    if (slot >= 0) {
+                        nvx = sv[slot];
+                        nvy = sv[strip_n + slot];
+                        nvz = sv[2 * strip_n + slot];
+                    } else if (!zone && plane_in && rw[h].in) {
+                        const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
+                        const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
+                        const float *c0 = R.center(s0, 0) + ci;
+                        const float dtxx_dx = t0[hi + 1] - t0[hi];
+                        const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
+                        const float dtyy_dy = R.center(sp, 0)[ci] - c0[0];
+                        const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
+                        const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
+                        const float dtxy_dx = txyc - t3[hi - 1];
+                        const float dtxz_dz = txzc - t4[hi - EFM_HX];
+                        const float dtxz_dx = txzc - t4[hi - 1];
+                        const float dtyz_dz = tyzc - t5[hi - EFM_HX];
+                        const float dtyz_dy = tyzc - R.halo(sm, 4)[hi];
+                        const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];
+                        const float bj = R.halo(sp, 5)[hi];
+                        const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
+                        const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
+                        const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
+                        const float k = H.k;
+                        nvx = c0[CF] + k * b_x * (dtxx_dx + dtxy_dy + dtxz_dz);
+                        nvy = c0[2 * CF] + k * b_y * (dtxy_dx + dtyy_dy + dtyz_dz);
+                        nvz = c0[3 * CF] + k * b_z * (dtxz_dx + dtyz_dy + dtzz_dz);
+                    }
+                    float *cw = R.center(s0, 1) + ci;
+                    cw[0] = nvx;
+                    cw[CF] = nvy;
+                    cw[2 * CF] = nvz;
                 }
-                if (slot >= 0) {
-                    nvx = sv[slot];
-                    nvy = sv[strip_n + slot];
-                    nvz = sv[2 * strip_n + slot];
-                } else if (!zone && plane_in && rw[h].in) {
-                    const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
-                    const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
-                    const float *c0 = R.center(s0, 0) + ci;
-                    const float dtxx_dx = t0[hi + 1] - t0[hi];
-                    const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
-                    const float dtyy_dy = R.center(sp, 0)[ci] - c0[0];
-                    const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
-                    const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
-                    const float dtxy_dx = txyc - t3[hi - 1];
-                    const float dtxz_dz = txzc - t4[hi - EFM_HX];
-                    const float dtxz_dx = txzc - t4[hi - 1];
-                    const float dtyz_dz = tyzc - t5[hi - EFM_HX];
-                    const float dtyz_dy = tyzc - R.halo(sm, 4)[hi];
-                    const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];
-                    const float bj = R.halo(sp, 5)[hi];
-                    const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
-                    const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
-                    const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
-                    const float k = H.k;
-                    nvx = c0[CF] + k * b_x * (dtxx_dx + dtxy_dy + dtxz_dz);
-                    nvy = c0[2 * CF] + k * b_y * (dtxy_dx + dtyy_dy + dtyz_dz);
-                    nvz = c0[3 * CF] + k * b_z * (dtxz_dx + dtyz_dy + dtzz_dz);
-                }
-                float *cw = R.center(s0, 1) + ci;
-                cw[0] = nvx;
-                cw[CF] = nvy;
-                cw[2 * CF] = nvz;
+                efm_fence_async_smem();
             }
-            efm_fence_async_smem();
-        } else if (mine) {
-            const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
+        } else {
+            // forward / adjoint: the plane's update, with or without the memory-variable code
+            auto plane = [&](auto tag) -> bool {
+                constexpr bool PML = decltype(tag)::value;
+                PsiPlane P{0, 0, 0, false};
+                float pp[ROWS][9];
+                if (PML) {
+                    P = psi_plane(H, j);
 #pragma unroll
-            for (int h = 0; h < ROWS; ++h) {
-                const int z = T.z0 + lr + 4 * h;
-                const bool guard = plane_in && rw[h].in;
-                const bool rec = rec_plane && colgrid[h] && efm_rec_bit(I, x, y, z);
-                if (!(guard || rec)) continue;
-                const int hi = rw[h].hidx, ci = rw[h].cidx;
-                float *cw = R.center(s0, 1) + ci;  // vx, vy, vz of this cell
-                float nvx = cw[0];
-                float nvy = cw[CF];
-                float nvz = cw[2 * CF];
-                if (guard) {
-                    const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
-                    const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
-                    const float dtxx_dx = t0[hi + 1] - t0[hi];
-                    const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
-                    const float dtyy_dy = R.center(sp, 0)[ci] - cw[-CF];
-                    const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
-                    const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
-                    const float dtxy_dx = txyc - t3[hi - 1];
-                    const float dtxz_dz = txzc - t4[hi - EFM_HX];
-                    const float dtxz_dx = txzc - t4[hi - 1];
-                    const float dtyz_dz = tyzc - t5[hi - EFM_HX];
-                    const float dtyz_dy = tyzc - R.halo(sm, 4)[hi];
-                    const float *p9 = pp[h];
-                    float q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f,
-                          q8 = 0.f, q9 = 0.f;
-                    if (rw[h].wx && rw[h].pxo >= 0) {
-                        const float a = cx_a, b = cx_b;
-                        q1 = b * p9[0] + a * dtxx_dx;
-                        q2 = b * p9[1] + a * dtxy_dx;
-                        q3 = b * p9[2] + a * dtxz_dx;
-                        H.psx[P.x + rw[h].pxo] = make_float4(q1, q2, q3, 0.f);
-                    }
-                    if (P.has_y) {
-                        const float a = cy_a, b = cy_b;
-                        q4 = b * p9[3] + a * dtyy_dy;
-                        q5 = b * p9[4] + a * dtxy_dy;
-                        q6 = b * p9[5] + a * dtyz_dy;
-                        H.psy[P.y + rw[h].pyo] = make_float4(q4, q5, q6, 0.f);
-                    }
-                    if (rw[h].wz && rw[h].pzo >= 0) {
-                        const float a = cz_a[h], b = cz_b[h];
-                        q7 = b * p9[6] + a * dtzz_dz;
-                        q8 = b * p9[7] + a * dtxz_dz;
-                        q9 = b * p9[8] + a * dtyz_dz;
-                        H.psz[P.z + rw[h].pzo] = make_float4(q7, q8, q9, 0.f);
-                    }
-                    // harmonic 2-point buoyancy from the precomputed 1/rho (:153-159)
-                    const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];
-                    const float bj = R.halo(sp, 5)[hi];
-                    const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
-                    const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
-                    const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
-                    const float k = H.k;
-                    nvx = nvx + k * b_x * ((dtxx_dx + q1) + (dtxy_dy + q5) + (dtxz_dz + q8));
-                    nvy = nvy + k * b_y * ((dtxy_dx + q2) + (dtyy_dy + q4) + (dtyz_dz + q9));
-                    nvz = nvz + k * b_z * ((dtxz_dx + q3) + (dtyz_dy + q6) + (dtzz_dz + q7));
+                    for (int h = 0; h < ROWS; ++h)
+                        if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
                 }
-                if (PASS == EFM_ADJ && rec) {
-                    const int tr = I.nt - 1 - it;
-                    const int64_t ntr = (int64_t)I.nt * I.nrec;
-                    const int c = x + nx * (z + nz * y);
-                    for (int q = efm_rec_find(I, c); q >= 0 && q < I.nrec && I.rec_lin[q] == c; ++q) {
-                        const int64_t o = (int64_t)tr * I.nrec + I.rec_id[q];
-                        nvx = __fadd_rn(nvx, I.res[o]);
-                        nvy = __fadd_rn(nvy, I.res[ntr + o]);
-                        nvz = __fadd_rn(nvz, I.res[2 * ntr + o]);
+                const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+                if (!mine) return false;
+                const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
+#pragma unroll
+                for (int h = 0; h < ROWS; ++h) {
+                    const int z = T.z0 + lr + 4 * h;
+                    const bool guard = plane_in && rw[h].in;
+                    const bool rec = rec_plane && colgrid[h] && efm_rec_bit(I, x, y, z);
+                    if (!(guard || rec)) continue;
+                    const int hi = rw[h].hidx, ci = rw[h].cidx;
+                    float *cw = R.center(s0, 1) + ci;  // vx, vy, vz of this cell
+                    float nvx = cw[0];
+                    float nvy = cw[CF];
+                    float nvz = cw[2 * CF];
+                    if (guard) {
+                        const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
+                        const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);
+                        const float dtxx_dx = t0[hi + 1] - t0[hi];
+                        const float dtzz_dz = t2[hi + EFM_HX] - t2[hi];
+                        const float dtyy_dy = R.center(sp, 0)[ci] - cw[-CF];
+                        const float txyc = t3[hi], txzc = t4[hi], tyzc = t5[hi];
+                        const float dtxy_dy = txyc - R.halo(sm, 2)[hi];
+                        const float dtxy_dx = txyc - t3[hi - 1];
+                        const float dtxz_dz = txzc - t4[hi - EFM_HX];
+                        const float dtxz_dx = txzc - t4[hi - 1];
+                        const float dtyz_dz = tyzc - t5[hi - EFM_HX];
+                        const float dtyz_dy = tyzc - R.halo(sm, 4)[hi];
+                        const float *p9 = pp[h];
+                        float q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f, q5 = 0.f, q6 = 0.f, q7 = 0.f,
+                              q8 = 0.f, q9 = 0.f;
+                        if (PML && rw[h].wx && rw[h].pxo >= 0) {
+                            const float a = cx_a, b = cx_b;
+                            q1 = b * p9[0] + a * dtxx_dx;
+                            q2 = b * p9[1] + a * dtxy_dx;
+                            q3 = b * p9[2] + a * dtxz_dx;
+                            H.psx[P.x + rw[h].pxo] = make_float4(q1, q2, q3, 0.f);
+                        }
+                        if (PML && P.has_y) {
+                            const float a = cy_a, b = cy_b;
+                            q4 = b * p9[3] + a * dtyy_dy;
+                            q5 = b * p9[4] + a * dtxy_dy;
+                            q6 = b * p9[5] + a * dtyz_dy;
+                            H.psy[P.y + rw[h].pyo] = make_float4(q4, q5, q6, 0.f);
+                        }
+                        if (PML && rw[h].wz && rw[h].pzo >= 0) {
+                            const float a = cz_a[h], b = cz_b[h];
+                            q7 = b * p9[6] + a * dtzz_dz;
+                            q8 = b * p9[7] + a * dtxz_dz;
+                            q9 = b * p9[8] + a * dtyz_dz;
+                            H.psz[P.z + rw[h].pzo] = make_float4(q7, q8, q9, 0.f);
+                        }
+                        // harmonic 2-point buoyancy from the precomputed 1/rho (:153-159)
+                        const float b0 = bu[hi], bi = bu[hi + 1], bk = bu[hi + EFM_HX];
+                        const float bj = R.halo(sp, 5)[hi];
+                        const float b_x = 2.f * b0 * bi * frcp(b0 + bi);
+                        const float b_y = 2.f * b0 * bj * frcp(b0 + bj);
+                        const float b_z = 2.f * b0 * bk * frcp(b0 + bk);
+                        const float k = H.k;
+                        nvx = nvx + k * b_x * ((dtxx_dx + q1) + (dtxy_dy + q5) + (dtxz_dz + q8));
+                        nvy = nvy + k * b_y * ((dtxy_dx + q2) + (dtyy_dy + q4) + (dtyz_dz + q9));
+                        nvz = nvz + k * b_z * ((dtxz_dx + q3) + (dtyz_dy + q6) + (dtzz_dz + q7));
                     }
-                }
-                cw[0] = nvx;
-                cw[CF] = nvy;
-                cw[2 * CF] = nvz;
-                if (PASS == EFM_FWD) {
-                    if (rec && I.gather != nullptr) {
+                    if (PASS == EFM_ADJ && rec) {
+                        const int tr = I.nt - 1 - it;
                         const int64_t ntr = (int64_t)I.nt * I.nrec;
                         const int c = x + nx * (z + nz * y);
                         for (int q = efm_rec_find(I, c); q >= 0 && q < I.nrec && I.rec_lin[q] == c; ++q) {
-                            const int64_t o = (int64_t)it * I.nrec + I.rec_id[q];
-                            I.gather[o] = nvx;
-                            I.gather[ntr + o] = nvy;
-                            I.gather[2 * ntr + o] = nvz;
+                            const int64_t o = (int64_t)tr * I.nrec + I.rec_id[q];
+                            nvx = __fadd_rn(nvx, I.res[o]);
+                            nvy = __fadd_rn(nvy, I.res[ntr + o]);
+                            nvz = __fadd_rn(nvz, I.res[2 * ntr + o]);
                         }
                     }
-                    if (border != nullptr && yin && sr[h].yf >= 0) {
-                        float *s = border + (int64_t)it * 3 * strip_n;
-                        auto put = [&](int sl) {
-                            s[sl] = nvx;
-                            s[strip_n + sl] = nvy;
-                            s[2 * strip_n + sl] = nvz;
-                        };
-                        if (sr[h].xf >= 0) put(sr[h].xf + yr * bz);
-                        if (yrow >= 0) put(sr[h].yf + yrow * bz * bx);
-                        if (sr[h].zf >= 0) put(sr[h].zf + yr * bx);
+                    cw[0] = nvx;
+                    cw[CF] = nvy;
+                    cw[2 * CF] = nvz;
+                    if (PASS == EFM_FWD) {
+                        if (rec && I.gather != nullptr) {
+                            const int64_t ntr = (int64_t)I.nt * I.nrec;
+                            const int c = x + nx * (z + nz * y);
+                            for (int q = efm_rec_find(I, c); q >= 0 && q < I.nrec && I.rec_lin[q] == c; ++q) {
+                                const int64_t o = (int64_t)it * I.nrec + I.rec_id[q];
+                                I.gather[o] = nvx;
+                                I.gather[ntr + o] = nvy;
+                                I.gather[2 * ntr + o] = nvz;
+                            }
+                        }
+                        if (border != nullptr && yin && sr[h].yf >= 0) {
+                            float *s = border + (int64_t)it * 3 * strip_n;
+                            auto put = [&](int sl) {
+                                s[sl] = nvx;
+                                s[strip_n + sl] = nvy;
+                                s[2 * strip_n + sl] = nvz;
+                            };
+                            if (sr[h].xf >= 0) put(sr[h].xf + yr * bz);
+                            if (yrow >= 0) put(sr[h].yf + yrow * bz * bx);
+                            if (sr[h].zf >= 0) put(sr[h].zf + yr * bx);
+                        }
                     }
                 }
-            }
-            if (store) efm_fence_async_smem();
+                if (store) efm_fence_async_smem();
+                return true;
+            };
+            bool wpml = ypml;  // warp-uniform: some lane of this warp has memory variables here
+#pragma unroll
+            for (int h = 0; h < ROWS; ++h) wpml = wpml || rw[h].wx || rw[h].wz;
+            mine = wpml ? plane(Tag<true>{}) : plane(Tag<false>{});
         }
         ok = __syncthreads_and(mine) != 0;
         if (!ok) break;

@@ -242,6 +242,17 @@ __device__ __forceinline__ void load_psi(const Hot &H, const PsiPlane &P, const 
     }
 }
 
+// Pull the next plane's memory variables of one row into L1 (no register, no wait); the
+// plane after the current one is then an L1 hit instead of an L2 round trip that the warp
+// would wait for right after the stage wait.
+__device__ __forceinline__ void prefetch_psi(const Hot &H, const PsiPlane &P, const Row &r) {
+    if (r.wx && r.pxo >= 0)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(H.psx + (P.x + r.pxo)));
+    if (P.has_y) asm volatile("prefetch.global.L1 [%0];" ::"l"(H.psy + (P.y + r.pyo)));
+    if (r.wz && r.pzo >= 0)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(H.psz + (P.z + r.pzo)));
+}
+
 // ------------------------------------------------------------------------------ stress
 // CPML coefficients of one cell, loaded once per block (x, z) or per plane (y)
 struct Coef {
@@ -459,6 +470,12 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
 #pragma unroll
                 for (int h = 0; h < ROWS; ++h)
                     if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
+                if (j + 1 < T.ye) {
+                    const PsiPlane Pn = psi_plane(H, j + 1);
+#pragma unroll
+                    for (int h = 0; h < ROWS; ++h)
+                        if (rw[h].in) prefetch_psi(H, Pn, rw[h]);
+                }
             }
             const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
             if (mine && plane_in) {
@@ -618,6 +635,12 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
 #pragma unroll
                     for (int h = 0; h < ROWS; ++h)
                         if (plane_in && rw[h].in) load_psi(H, P, rw[h], pp[h]);
+                    if (j + 1 < T.ye) {
+                        const PsiPlane Pn = psi_plane(H, j + 1);
+#pragma unroll
+                        for (int h = 0; h < ROWS; ++h)
+                            if (rw[h].in) prefetch_psi(H, Pn, rw[h]);
+                    }
                 }
                 const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
                 if (!mine) return false;

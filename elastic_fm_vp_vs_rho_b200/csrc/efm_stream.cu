@@ -570,29 +570,51 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
         const bool store = PASS == EFM_REV || plane_in || rec_plane;
         bool mine;
         if (PASS == EFM_REV) {
+            // reverse rebuild (-dt, no CPML) into the ping-pong partner f.vo: CPML slabs -> 0,
+            // boundary strips -> the values saved at forward step nt-2-it (:1955-1960),
+            // box interior -> stencil update, never-updated cells -> 0.  The strip values of
+            // this plane are requested before the stage wait, the next plane's pulled into L1.
+            const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
+            // first strip slot of row h on plane y (its three families hold the same values)
+            auto slot_of = [&](int h, int y) -> int {
+                const int r = y - W;
+                if (zone_xz[h] || y < W || y >= ny - W || r >= by || sr[h].yf < 0) return -1;
+                if (sr[h].xf >= 0) return sr[h].xf + r * bz;
+                const int row = r < 2 ? r : (r >= by - 2 ? 2 + (r - (by - 2)) : -1);
+                if (row >= 0) return sr[h].yf + row * bz * bx;
+                if (sr[h].zf >= 0) return sr[h].zf + r * bx;
+                return -1;
+            };
+            int slot[ROWS];
+            float sval[ROWS][3];
+#pragma unroll
+            for (int h = 0; h < ROWS; ++h) {
+                slot[h] = colgrid[h] ? slot_of(h, j) : -1;
+                if (slot[h] >= 0) {
+                    sval[h][0] = sv[slot[h]];
+                    sval[h][1] = sv[strip_n + slot[h]];
+                    sval[h][2] = sv[2 * strip_n + slot[h]];
+                }
+                const int sn = j + 1 < T.ye && colgrid[h] ? slot_of(h, j + 1) : -1;
+                if (sn >= 0) {
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(sv + sn));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(sv + strip_n + sn));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(sv + 2 * strip_n + sn));
+                }
+            }
             mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
             if (mine) {
-                // reverse rebuild (-dt, no CPML) into the ping-pong partner f.vo: CPML slabs -> 0,
-                // boundary strips -> the values saved at forward step nt-2-it (:1955-1960),
-                // box interior -> stencil update, never-updated cells -> 0
                 const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
-                const float *sv = border + (int64_t)(I.nt - 2 - it) * 3 * strip_n;
 #pragma unroll
                 for (int h = 0; h < ROWS; ++h) {
                     if (!colgrid[h]) continue;
                     const int hi = rw[h].hidx, ci = rw[h].cidx;
                     float nvx = 0.f, nvy = 0.f, nvz = 0.f;
                     const bool zone = zone_xz[h] || ypml;
-                    int slot = -1;
-                    if (!zone && yin && sr[h].yf >= 0) {
-                        if (sr[h].xf >= 0) slot = sr[h].xf + yr * bz;
-                        else if (yrow >= 0) slot = sr[h].yf + yrow * bz * bx;
-                        else if (sr[h].zf >= 0) slot = sr[h].zf + yr * bx;
-                    }
-                    if (slot >= 0) {
-                        nvx = sv[slot];
-                        nvy = sv[strip_n + slot];
-                        nvz = sv[2 * strip_n + slot];
+                    if (slot[h] >= 0) {
+                        nvx = sval[h][0];
+                        nvy = sval[h][1];
+                        nvz = sval[h][2];
                     } else if (!zone && plane_in && rw[h].in) {
                         const float *t0 = R.halo(s0, 0), *t2 = R.halo(s0, 1), *t3 = R.halo(s0, 2);
                         const float *t4 = R.halo(s0, 3), *t5 = R.halo(s0, 4), *bu = R.halo(s0, 5);

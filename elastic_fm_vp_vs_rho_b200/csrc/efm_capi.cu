@@ -65,6 +65,7 @@ struct Inst {
     float *cpml = nullptr;
     uint32_t *rec_mask = nullptr;
     int *rec_lin = nullptr, *rec_id = nullptr;
+    int *rec_wfirst = nullptr;    // per mask word: first sorted entry of its cells, or -1
     uint8_t *rec_tile = nullptr;  // [ny][tiles_z][tiles_x] of the streaming layout
     float *aux = nullptr;         // 1/mu, 1/rho
     float *fields = nullptr;  // va(3) t(6) | vb(3) bv(3) bt(6) when gradient-capable
@@ -389,6 +390,7 @@ void free_inst(Inst &I) {
     cudaFree(I.rec_mask);
     cudaFree(I.rec_lin);
     cudaFree(I.rec_id);
+    cudaFree(I.rec_wfirst);
     cudaFree(I.rec_tile);
     cudaFree(I.aux);
     cudaFree(I.fields);
@@ -401,7 +403,7 @@ void free_inst(Inst &I) {
     I.ck_every = I.nck = 0;
     I.cpml = nullptr;
     I.rec_mask = nullptr;
-    I.rec_lin = I.rec_id = nullptr;
+    I.rec_lin = I.rec_id = I.rec_wfirst = nullptr;
     I.rec_tile = nullptr;
     I.aux = nullptr;
     I.fields = I.psi = I.border = nullptr;
@@ -536,6 +538,7 @@ EfmInst base_table(const Inst &I) {
     d.rec_mask = I.rec_mask;
     d.rec_lin = I.rec_lin;
     d.rec_id = I.rec_id;
+    d.rec_wfirst = I.rec_wfirst;
     d.strip_n = I.strip_n;
     return d;
 }
@@ -972,6 +975,22 @@ int efm_add_instance(efm_ctx *ctx, const efm_instance_desc *d, int *id) {
         lin[r] = lr[r].first;
         rid[r] = lr[r].second;
     }
+    // per mask word: index of the first sorted entry whose cell lies in the word (entries of
+    // earlier words counted), so a cell's entry is that plus the set bits below it; -1 for a
+    // word holding a cell with several receivers (those cells search the sorted list)
+    std::vector<int> wfirst(mask.size(), 0);
+    {
+        std::vector<int> cnt(mask.size() + 1, 0);
+        auto word = [&](int c) {
+            const int x = c % I.nx, rest = c / I.nx;
+            return (size_t)rest * nw + (x >> 5);  // rest = z + nz*y
+        };
+        for (int r = 0; r < I.nrec; ++r) cnt[word(lin[r]) + 1] += 1;
+        for (size_t w = 0; w < mask.size(); ++w) cnt[w + 1] += cnt[w];
+        for (size_t w = 0; w < mask.size(); ++w) wfirst[w] = cnt[w];
+        for (int r = 1; r < I.nrec; ++r)
+            if (lin[r] == lin[r - 1]) wfirst[word(lin[r])] = -1;
+    }
     auto bad = [&](cudaError_t e) {
         free_inst(I);
         return fail(EFM_ERR_CUDA, std::string("instance upload: ") + cudaGetErrorString(e));
@@ -981,10 +1000,13 @@ int efm_add_instance(efm_ctx *ctx, const efm_instance_desc *d, int *id) {
     if ((e = cudaMalloc(&I.rec_mask, mask.size() * sizeof(uint32_t)))) return bad(e);
     if ((e = cudaMalloc(&I.rec_lin, I.nrec * sizeof(int)))) return bad(e);
     if ((e = cudaMalloc(&I.rec_id, I.nrec * sizeof(int)))) return bad(e);
+    if ((e = cudaMalloc(&I.rec_wfirst, wfirst.size() * sizeof(int)))) return bad(e);
     if ((e = cudaMemcpy(I.cpml, I.cpml_host.data(), nc * sizeof(float), cudaMemcpyHostToDevice))) return bad(e);
     if ((e = cudaMemcpy(I.rec_mask, mask.data(), mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice))) return bad(e);
     if ((e = cudaMemcpy(I.rec_lin, lin.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
     if ((e = cudaMemcpy(I.rec_id, rid.data(), I.nrec * sizeof(int), cudaMemcpyHostToDevice))) return bad(e);
+    if ((e = cudaMemcpy(I.rec_wfirst, wfirst.data(), wfirst.size() * sizeof(int), cudaMemcpyHostToDevice)))
+        return bad(e);
     {
         const int tx = (I.nx + EFM_STX - 1) / EFM_STX, tz = (I.nz + EFM_REC_TZ - 1) / EFM_REC_TZ;
         std::vector<uint8_t> rt((size_t)I.ny * tz * tx, 0);

@@ -59,6 +59,7 @@ struct EfmInst {
     const uint32_t *rec_mask;  // one bit per cell: [ny][nz][ceil(nx/32)] words
     const int *rec_lin;        // receiver cells, sorted linear index
     const int *rec_id;         // receiver number of each sorted entry
+    const int *rec_wfirst;     // per rec_mask word: first sorted entry of its cells, -1: repeats
     float *gather;     // [3][nt][nrec] forward record, or null
     const float *res;  // [3][nt][nrec] adjoint source, or null
     float *border;     // [nt][3][strip_n] boundary strips, or null
@@ -135,6 +136,22 @@ __device__ __forceinline__ int efm_rec_find(const EfmInst &I, int c) {
         if (I.rec_lin[mid] < c) lo = mid + 1; else hi = mid;
     }
     return (lo < I.nrec && I.rec_lin[lo] == c) ? lo : -1;
+}
+
+// First sorted entry of the receivers at cell (x, y, z), or -1 if there are none, from the
+// cell's mask word and the word's first entry (two independent loads) plus the set bits
+// below the cell; *more is set when the cell may hold several receivers (then the entries
+// q, q+1, ... with rec_lin[q] == cell all belong to it).
+__device__ __forceinline__ int efm_rec_first(const EfmInst &I, int x, int y, int z, bool *more) {
+    const int nw = (I.nx + 31) >> 5;
+    const int64_t wi = ((int64_t)y * I.nz + z) * nw + (x >> 5);
+    const uint32_t w = __ldg(&I.rec_mask[wi]);
+    const int f = __ldg(&I.rec_wfirst[wi]);
+    *more = false;
+    if (!((w >> (x & 31)) & 1u)) return -1;
+    if (f >= 0) return f + __popc(w & ((1u << (x & 31)) - 1u));
+    *more = true;
+    return efm_rec_find(I, x + I.nx * (z + I.nz * y));
 }
 
 __device__ __forceinline__ bool efm_rec_bit(const EfmInst &I, int x, int y, int z) {

@@ -671,7 +671,9 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                 for (int h = 0; h < ROWS; ++h) {
                     const int z = T.z0 + lr + 4 * h;
                     const bool guard = plane_in && rw[h].in;
-                    const bool rec = rec_plane && colgrid[h] && efm_rec_bit(I, x, y, z);
+                    bool more = false;  // the cell may hold several receivers
+                    const int rq = rec_plane && colgrid[h] ? efm_rec_first(I, x, y, z, &more) : -1;
+                    const bool rec = rq >= 0;
                     if (!(guard || rec)) continue;
                     const int hi = rw[h].hidx, ci = rw[h].cidx;
                     float *cw = R.center(s0, 1) + ci;  // vx, vy, vz of this cell
@@ -730,11 +732,12 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                         const int tr = I.nt - 1 - it;
                         const int64_t ntr = (int64_t)I.nt * I.nrec;
                         const int c = x + nx * (z + nz * y);
-                        for (int q = efm_rec_find(I, c); q >= 0 && q < I.nrec && I.rec_lin[q] == c; ++q) {
+                        for (int q = rq;;) {
                             const int64_t o = (int64_t)tr * I.nrec + I.rec_id[q];
                             nvx = __fadd_rn(nvx, I.res[o]);
                             nvy = __fadd_rn(nvy, I.res[ntr + o]);
                             nvz = __fadd_rn(nvz, I.res[2 * ntr + o]);
+                            if (!more || ++q >= I.nrec || I.rec_lin[q] != c) break;
                         }
                     }
                     cw[0] = nvx;
@@ -744,11 +747,12 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                         if (rec && I.gather != nullptr) {
                             const int64_t ntr = (int64_t)I.nt * I.nrec;
                             const int c = x + nx * (z + nz * y);
-                            for (int q = efm_rec_find(I, c); q >= 0 && q < I.nrec && I.rec_lin[q] == c; ++q) {
+                            for (int q = rq;;) {
                                 const int64_t o = (int64_t)it * I.nrec + I.rec_id[q];
                                 I.gather[o] = nvx;
                                 I.gather[ntr + o] = nvy;
                                 I.gather[2 * ntr + o] = nvz;
+                                if (!more || ++q >= I.nrec || I.rec_lin[q] != c) break;
                             }
                         }
                         if (border != nullptr && yin && sr[h].yf >= 0) {

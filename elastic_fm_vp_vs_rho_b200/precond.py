@@ -14,9 +14,10 @@ model to a model update:
              BF16 tcgen05 kernels of efm_conv.cu with FP32 accumulation)
     output:  channels 0-2 = the update direction for (Vp, Vs, rho) in normalised units.
 
-Training pairs come from plain L-BFGS runs on seeded random models (the accepted update of
-each iteration, scaled to unit maximum); the loss is the mean squared error over the three
-used channels; Adam on FP32 master weights.
+Training pairs come from plain L-BFGS runs on seeded random models: the features of each
+iterate and, as target, either GAIN x (true - current) normalised model ("error", the
+default) or the accepted L-BFGS update scaled to unit maximum ("update"); the loss is the
+mean squared error over the three used channels; Adam on FP32 master weights.
 
 :func:`invert` runs an inversion with either plain L-BFGS or the learned direction; every
 learned direction must pass a descent test (g . d < 0) and an Armijo backtracking line

@@ -393,6 +393,14 @@ def main():
                 else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": alg[dom], "traffic": traffic,
                 "per_kernel": per}
+    # the whole step: algorithmic bytes of every launch of one step (launch counts from the
+    # statistics pass) over the timed step's device time, overlap between launches included
+    step_bytes = sum(alg[name] * launches[k] / stat_steps
+                     for k, name in enumerate(_lib.KERNEL_NAMES) if launches[k] and name in alg)
+    step_gbs = step_bytes / (total_ms / args.steps * 1e-3) / 1e9
+    roofline["whole_step"] = {"algorithmic_bytes_per_step": step_bytes, "achieved": step_gbs,
+                              "frac": step_gbs / peak,
+                              "bytes_per_cell_update": step_bytes / upd}
 
     e2e = None
     if not args.no_e2e:

@@ -90,6 +90,7 @@ SIGNATURES = {
     "efm_gather_offset": (_L, [_P, _I]),
     "efm_workspace_bytes": (_L, [_P, _I]),
     "efm_forward": (_I, [_P, _P, _I, _P]),
+    "efm_forward_illumination": (_I, [_P, _P, _I, _P, _P]),
     "efm_gradient": (_I, [_P, _P, _P, _P, _I, _P]),
     "efm_residual_misfit": (_I, [_P, _P, _P, _P, _P, _P]),
     "efm_residual_misfit_noalloc": (_I, [_P, _P, _P, _P, _I, _P, _P]),

@@ -589,7 +589,7 @@ int ensure_exact(efm_ctx *ctx) {
 
 // Forward tables (slots T_FWD_S, T_FWD_V) and tensor maps; gathers / strips optional.
 int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cudaStream_t s,
-                    bool *stream_kernels) {
+                    bool *stream_kernels, float *illum = nullptr) {
     int rc;
     const int n = (int)ctx->inst.size();
     const bool st = stream_ok(ctx);
@@ -611,6 +611,7 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
         for (int c = 0; c < 3; ++c) d.f.v[c] = d.f.vo[c] = I.va(c);
         for (int c = 0; c < 6; ++c) d.f.t[c] = I.tt(c);
         d.gather = gathers ? gathers + I.gather_off : nullptr;
+        d.illum = illum ? illum + I.grad_off / 3 : nullptr;  // one volume per instance
         d.border = strips ? I.border : nullptr;
         EfmInst ds = d, dv = d;
         if (st) {
@@ -658,7 +659,7 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
     return EFM_OK;
 }
 
-int forward_step(efm_ctx *ctx, bool st, int it, cudaStream_t s) {
+int forward_step(efm_ctx *ctx, bool st, int it, cudaStream_t s, bool illum = false) {
     const int n = (int)ctx->inst.size();
     const EfmInst *ts = ctx->d_tab, *tv = ctx->d_tab + n;
     int rc;
@@ -668,7 +669,8 @@ int forward_step(efm_ctx *ctx, bool st, int it, cudaStream_t s) {
          })))
         return rc;
     return timed_launch(ctx, EFM_K_FWD_VELOCITY, s, [&] {
-        return st ? efm_launch_stream(EFM_FWD, 1, ctx->rows, ctx->ring, tv, n, ctx->tiles[T_FWD_V], it, s)
+        return st ? efm_launch_stream(EFM_FWD, illum ? 2 : 1, ctx->rows, ctx->ring, tv, n,
+                                      ctx->tiles[T_FWD_V], it, s)
                   : efm_launch_velocity(EFM_FWD, tv, n, ctx->tiles[T_FWD_V], it, s);
     });
 }
@@ -1070,6 +1072,10 @@ int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders) {
 }
 
 int efm_forward(efm_ctx *ctx, float *gathers, int save, void *stream) {
+    return efm_forward_illumination(ctx, gathers, save, nullptr, stream);
+}
+
+int efm_forward_illumination(efm_ctx *ctx, float *gathers, int save, float *illum, void *stream) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (gathers == nullptr) return fail(EFM_ERR_ARG, "null gathers");
@@ -1078,7 +1084,7 @@ int efm_forward(efm_ctx *ctx, float *gathers, int save, void *stream) {
     if ((rc = ensure_workspace(ctx, strips || ckpts, strips))) return rc;
     if (ckpts && (rc = ensure_exact(ctx))) return rc;
     bool st = false;
-    if ((rc = prepare_forward(ctx, gathers, strips, true, s, &st))) return rc;
+    if ((rc = prepare_forward(ctx, gathers, strips, true, s, &st, illum))) return rc;
     int maxnt = 0;
     for (Inst &I : ctx->inst) {
         maxnt = std::max(maxnt, I.nt);
@@ -1087,7 +1093,7 @@ int efm_forward(efm_ctx *ctx, float *gathers, int save, void *stream) {
     }
     std::vector<int64_t> key = {st, ctx->rows, ctx->ring, ctx->opt_pdl, (int64_t)ctx->inst.size(),
                                 maxnt, (int64_t)(uintptr_t)ctx->d_tab, ctx->tiles[T_FWD_S],
-                                ctx->tiles[T_FWD_V], ckpts};
+                                ctx->tiles[T_FWD_V], ckpts, illum != nullptr};
     if (ckpts)
         for (const Inst &I : ctx->inst)
             key.insert(key.end(), {I.ck_every, I.nt, (int64_t)(uintptr_t)I.ckpt,
@@ -1096,7 +1102,7 @@ int efm_forward(efm_ctx *ctx, float *gathers, int save, void *stream) {
     rc = run_loop(ctx, 0, key, s, [&](cudaStream_t ls) {
         int r;
         for (int it = 0; it < maxnt; ++it) {
-            if ((r = forward_step(ctx, st, it, ls))) return r;
+            if ((r = forward_step(ctx, st, it, ls, illum != nullptr))) return r;
             if (ckpts)
                 for (Inst &I : ctx->inst)
                     if ((it + 1) % I.ck_every == 0 && it + 1 < I.nt) {

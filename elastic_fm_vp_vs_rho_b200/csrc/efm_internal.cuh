@@ -61,6 +61,7 @@ struct EfmInst {
     const int *rec_id;         // receiver number of each sorted entry
     const int *rec_wfirst;     // per rec_mask word: first sorted entry of its cells, -1: repeats
     float *gather;     // [3][nt][nrec] forward record, or null
+    float *illum;      // forward illumination accumulator (sum over steps of |v|^2), or null
     const float *res;  // [3][nt][nrec] adjoint source, or null
     float *border;     // [nt][3][strip_n] boundary strips, or null
     int64_t strip_n;

@@ -265,6 +265,7 @@ efm_velocity_kernel(const EfmInst *__restrict__ insts, int ninst, int it) {
     ox[c] = nvx; oy[c] = nvy; oz[c] = nvz;
 
     if (PASS == EFM_FWD) {
+        if (I.illum != nullptr) I.illum[c] += nvx * nvx + nvy * nvy + nvz * nvz;
         if (I.gather != nullptr && efm_rec_bit(I, x, y, z)) {
             const int64_t ntr = (int64_t)I.nt * I.nrec;
             for (int j = efm_rec_find(I, (int)c); j >= 0 && j < I.nrec && I.rec_lin[j] == (int)c; ++j) {

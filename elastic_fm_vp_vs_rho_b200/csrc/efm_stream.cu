@@ -508,7 +508,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
 
 // halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint);
 // the rebuild stores its new velocity through three more maps (tm[NH + NC ..]) into f.vo
-template <int PASS, int ROWS, int SR>
+template <int PASS, int ROWS, int SR, bool ILLUM = false>
 __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts, int ninst, int it,
                                               int block, unsigned char *smem) {
     constexpr int NH = 6, NC = 4;
@@ -529,6 +529,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     const unsigned long long recbits = s_rec;
     const Hot H = make_hot(I, 1);
     float *const border = I.border;
+    float *const illum = ILLUM ? I.illum : nullptr;
     const int64_t strip_n = I.strip_n;
     const int by = ny - 2 * W, bx = nx - 2 * W, bz = nz - W - 2;
     Row rw[ROWS];
@@ -744,6 +745,9 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     cw[CF] = nvy;
                     cw[2 * CF] = nvz;
                     if (PASS == EFM_FWD) {
+                        // cells the stencil never updates keep v = 0 and add nothing
+                        if (ILLUM && guard)
+                            illum[x + nx * (z + nz * y)] += nvx * nvx + nvy * nvy + nvz * nvz;
                         if (rec && I.gather != nullptr) {
                             const int64_t ntr = (int64_t)I.nt * I.nrec;
                             const int c = x + nx * (z + nz * y);
@@ -797,6 +801,14 @@ __global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
 efm_velocity_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     extern __shared__ __align__(1024) unsigned char smem[];
     velocity_body<PASS, ROWS, SR>(insts, ninst, it, blockIdx.x, smem);
+}
+
+// Forward velocity that also sums |v|^2 into the table's illumination volume.
+template <int ROWS, int SR>
+__global__ void __launch_bounds__(EFM_STHREADS, efm_stream_blocks(ROWS, SR))
+efm_velocity_illum_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    velocity_body<EFM_FWD, ROWS, SR, true>(insts, ninst, it, blockIdx.x, smem);
 }
 
 // Two independent half-steps in one launch: blocks [0, tiles_s) run the stress pass PS of
@@ -886,6 +898,8 @@ static void launch_rows(int pass, int kind, const EfmInst *insts, int ninst, int
             case EFM_ADJ: launch_k(efm_stress_stream<EFM_ADJ, ROWS, SR>, tiles, SS, s, insts, ninst, it); break;
             default: launch_k(efm_stress_stream<EFM_REV, ROWS, SR>, tiles, SS, s, insts, ninst, it); break;
         }
+    } else if (kind == 2) {
+        launch_k(efm_velocity_illum_stream<ROWS, SR>, tiles, SV, s, insts, ninst, it);
     } else {
         switch (pass) {
             case EFM_FWD: launch_k(efm_velocity_stream<EFM_FWD, ROWS, SR>, tiles, SV, s, insts, ninst, it); break;
@@ -920,8 +934,9 @@ extern "C" cudaError_t efm_launch_pair(int which, int rows, int ring, const EfmI
     return take_launch_err();
 }
 
-// kind 0 = stress, 1 = velocity; rows = cells per thread (1 or 2) and ring = stages (4, or
-// 6 with one row), matching the tile layout and tensor-map boxes the table was built with.
+// kind 0 = stress, 1 = velocity, 2 = forward velocity that also sums the illumination;
+// rows = cells per thread (1 or 2) and ring = stages (4, or 6 with one row), matching the
+// tile layout and tensor-map boxes the table was built with.
 extern "C" cudaError_t efm_launch_stream(int pass, int kind, int rows, int ring,
                                          const EfmInst *insts, int ninst, int tiles, int it,
                                          cudaStream_t s) {
@@ -953,6 +968,7 @@ static cudaError_t set_rows_attributes() {
     if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_FWD, ROWS, SR>, A, sv))) return e;
     if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_ADJ, ROWS, SR>, A, sv))) return e;
     if ((e = cudaFuncSetAttribute(efm_velocity_stream<EFM_REV, ROWS, SR>, A, sv))) return e;
+    if ((e = cudaFuncSetAttribute(efm_velocity_illum_stream<ROWS, SR>, A, sv))) return e;
     const int sp = ss > sv ? ss : sv;
     if ((e = cudaFuncSetAttribute(efm_pair_stream<EFM_ADJ, EFM_REV, ROWS, SR>, A, sp))) return e;
     return cudaFuncSetAttribute(efm_pair_stream<EFM_REV, EFM_ADJ, ROWS, SR>, A, sp);

@@ -194,21 +194,40 @@ class ShotBatch:
         inf = self.infos[i]
         return buf[off:off + 3 * inf.ncell].view(3, *inf.shape)
 
+    @property
+    def illum_size(self) -> int:
+        """Floats of an illumination buffer: one (ny, nz, nx) volume per instance."""
+        return sum(inf.ncell for inf in self.infos)
+
+    def illum_view(self, buf, i):
+        """(ny, nz, nx) view of instance i inside an illumination buffer."""
+        off = sum(inf.ncell for inf in self.infos[:i])
+        inf = self.infos[i]
+        return buf[off:off + inf.ncell].view(*inf.shape)
+
     def workspace_bytes(self, save_borders=True) -> int:
         return int(self._L.efm_workspace_bytes(self._ctx, 1 if save_borders else 0))
 
     # ------------------------------------------------------------------ compute
-    def forward(self, save_borders=False, checkpoints=False, out=None, stream=None):
+    def forward(self, save_borders=False, checkpoints=False, out=None, illum=None, stream=None):
         """Forward-model every instance; returns the gather buffer (float32, gather layout).
 
         save_borders: keep the boundary strips the reference-mode gradient rebuilds from;
-        checkpoints: keep full-state checkpoints for the exact gradient."""
+        checkpoints: keep full-state checkpoints for the exact gradient;
+        illum: float32 CUDA buffer of illum_size floats into which the forward illumination
+        sum_t |v|^2 of every instance is added (efm_forward_illumination; zero it first)."""
         import torch
         if out is None:
             out = torch.empty(self.gather_size, dtype=torch.float32, device="cuda")
         save = (EFM_SAVE_STRIPS if save_borders else 0) | (EFM_SAVE_CHECKPOINTS if checkpoints else 0)
         with _range("efm_forward"):
-            check(self._L.efm_forward(self._ctx, ptr(out), save, stream_ptr(stream)))
+            if illum is None:
+                check(self._L.efm_forward(self._ctx, ptr(out), save, stream_ptr(stream)))
+            else:
+                if illum.dtype != torch.float32 or illum.numel() < self.illum_size or not illum.is_cuda:
+                    raise ValueError("illum must be a float32 CUDA buffer of illum_size floats")
+                check(self._L.efm_forward_illumination(self._ctx, ptr(out), save, ptr(illum),
+                                                       stream_ptr(stream)))
         return out
 
     def residual_misfit(self, mod, obs, res=None, stream=None):

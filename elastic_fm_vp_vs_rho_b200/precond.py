@@ -9,7 +9,11 @@ model to a model update:
         0-2  gradient of the misfit w.r.t. (Vp, Vs, rho) in normalised units, each scaled
              by its largest magnitude
         3-5  the normalised model (value / mean - 1)
-        6    depth z / nz (geometric spreading / illumination falls with depth)
+        6    depth z / nz (geometric spreading falls with depth)
+        7    with illumination=True: forward illumination of the current model, sum over
+             shots and steps of |v|^2 (efm_forward_illumination), as
+             log10(I / max I + 1e-4) / 4 + 1 in [0, 1] -- the diagonal a pseudo-Hessian
+             preconditioner would divide by; zero otherwise
     network: conv3d 16->32, ReLU, 32->64, ReLU, 64->32, ReLU, 32->16 (3x3x3, zero padding;
              BF16 tcgen05 kernels of efm_conv.cu with FP32 accumulation)
     output:  channels 0-2 = the update direction for (Vp, Vs, rho) in normalised units.
@@ -35,7 +39,7 @@ import numpy as np
 from . import conv3d
 
 WIDTHS = (16, 32, 64, 32, 16)
-NFEAT = 7
+NFEAT = 8
 GAIN = 10.0  # "error" targets: network output = GAIN x (normalised true model - current)
 
 
@@ -138,8 +142,9 @@ class PreconditionerNet:
             self.prep()
 
 
-def features(g3, p3):
-    """(3, ny, nz, nx) gradient and normalised model -> (ny, nz, nx, 16) BF16 features."""
+def features(g3, p3, illum=None):
+    """(3, ny, nz, nx) gradient and normalised model (and the (ny, nz, nx) forward
+    illumination, channel 7 stays zero without it) -> (ny, nz, nx, 16) BF16 features."""
     import torch
     _, ny, nz, nx = g3.shape
     f = torch.zeros((ny, nz, nx, WIDTHS[0]), dtype=torch.float32, device=g3.device)
@@ -148,6 +153,9 @@ def features(g3, p3):
         f[..., c] = g3[c] / s
         f[..., 3 + c] = p3[c] - 1.0
     f[..., 6] = (torch.arange(nz, device=g3.device, dtype=torch.float32) / nz)[None, :, None]
+    if illum is not None:
+        rel = illum.float() / illum.max().clamp_min(1e-30)
+        f[..., 7] = torch.log10(rel + 1e-4) / 4.0 + 1.0
     return f.to(torch.bfloat16).contiguous()
 
 
@@ -201,11 +209,13 @@ class InversionProblem:
     """Seeded true / initial model, earthquake-style MT sources at depth and surface
     receivers; misfit and exact gradient evaluations through one ShotBatch."""
 
-    def __init__(self, spec: ProblemSpec):
+    def __init__(self, spec: ProblemSpec, illumination=False):
         import torch
         from . import configs
         from .engine import ShotBatch
         s = self.spec = spec
+        self.use_illum = illumination
+        self.illum = None  # forward illumination at the model of the last gradient call
         rng = np.random.default_rng(spec.seed)
         vp, vs, rho = configs.layered_anomaly_model(s.ny, s.nz, s.nx, s.dx, spec.seed,
                                                     n_layers=4, n_anomalies=3, sigma_m=60.0,
@@ -265,11 +275,15 @@ class InversionProblem:
         from .engine import chain_rule, smooth_mask
         m = p * self.scale
         self._set(m)
-        mod = self.batch.forward(checkpoints=True)
+        ill = (torch.zeros(self.batch.illum_size, dtype=torch.float32, device="cuda")
+               if self.use_illum else None)
+        mod = self.batch.forward(checkpoints=True, illum=ill)
         res, mis = self.batch.residual_misfit(mod, self.obs)
         g, _ = self.batch.gradient(res, exact=True)
         self.solves += 2
         s = self.spec
+        if ill is not None:
+            self.illum = ill.view(len(self.srcs), s.ny, s.nz, s.nx).sum(dim=0)
         n = s.nx * s.ny * s.nz
         gv = g.reshape(len(self.srcs), 3, s.ny, s.nz, s.nx).sum(dim=0).contiguous()
         gl, gm, gr = gv[0].contiguous(), gv[1].contiguous(), gv[2].contiguous()
@@ -363,7 +377,7 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="error", 
         used = None
         step = None
         if net is not None and (learned_iters is None or it <= learned_iters):
-            out = net.forward(features(g, p))
+            out = net.forward(features(g, p, prob.illum))
             d = out[..., :3].permute(3, 0, 1, 2).contiguous()
             dmax = float(d.abs().max())
             if net.target == "error":
@@ -393,7 +407,7 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="error", 
         if record is not None:
             t = ((prob.true / prob.scale - p) * GAIN if target == "error"
                  else step / step.abs().max())
-            record.append((features(g, p), t.permute(1, 2, 3, 0).contiguous()))
+            record.append((features(g, p, prob.illum), t.permute(1, 2, 3, 0).contiguous()))
         p_new = p + step
         J_new, g_new = prob.gradient(p_new)
         lb.update(step, g_new - g)
@@ -418,7 +432,7 @@ POLICIES = {"always": dict(learned_iters=None), "first2": dict(learned_iters=2),
 
 
 def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=12, epochs=40,
-               spec=None, target="error", log=None):
+               spec=None, target="error", log=None, illumination=False):
     """Train on plain-L-BFGS runs of seeded models, then, on unseen seeds, compare plain
     L-BFGS with each learned policy: the solves each needs to reach plain L-BFGS's final
     misfit (None: not reached within `iters` iterations)."""
@@ -427,7 +441,7 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
     samples = []
     t0 = time.time()
     for s in train_seeds:
-        prob = InversionProblem(dataclasses.replace(base, seed=s))
+        prob = InversionProblem(dataclasses.replace(base, seed=s), illumination)
         invert(prob, iters, record=samples, target=target)
         prob.batch.close()
     t_data = time.time() - t0
@@ -437,7 +451,7 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
     t_train = time.time() - t0
     tests = []
     for ts in test_seeds:
-        prob = InversionProblem(dataclasses.replace(base, seed=ts))
+        prob = InversionProblem(dataclasses.replace(base, seed=ts), illumination)
         plain = invert(prob, iters, log=log)
         target_j = plain[-1]["misfit"]
         row = dict(seed=ts, target_misfit=target_j, solves_plain=plain[-1]["solves"],
@@ -455,7 +469,8 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
         r = [t["solves_plain"] / t["policies"][name]["solves"] if t["policies"][name]["solves"]
              else 0.0 for t in tests]
         summary[name] = dict(solve_ratio_per_seed=r, reached=sum(x > 0 for x in r))
-    return dict(spec=dataclasses.asdict(base), target=target, train_seeds=list(train_seeds),
+    return dict(spec=dataclasses.asdict(base), target=target, illumination=illumination,
+                train_seeds=list(train_seeds),
                 test_seeds=list(test_seeds), iters=iters, epochs=epochs, n_samples=len(samples),
                 loss_first=losses[0], loss_last=losses[-1], data_s=t_data, train_s=t_train,
                 summary=summary, tests=tests)
@@ -474,13 +489,16 @@ if __name__ == "__main__":
     ap.add_argument("--nt", type=int, default=320)
     ap.add_argument("--shots", type=int, default=4)
     ap.add_argument("--receivers", type=int, default=8, help="per side of the surface grid")
+    ap.add_argument("--illumination", action="store_true",
+                    help="fill feature channel 7 with the forward illumination")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
     gx, gy, gz = (int(v) for v in a.grid.split(","))
     spec = ProblemSpec(nx=gx, ny=gy, nz=gz, nt=a.nt, nshots=a.shots, nrec=a.receivers)
     r = experiment(train_seeds=tuple(range(100, 100 + a.train)),
                    test_seeds=tuple(int(v) for v in a.test_seeds.split(",")),
-                   iters=a.iters, epochs=a.epochs, spec=spec, target=a.target, log=print)
+                   iters=a.iters, epochs=a.epochs, spec=spec, target=a.target, log=print,
+                   illumination=a.illumination)
     s = json.dumps(r, indent=1)
     if a.out:
         with open(a.out, "w") as f:

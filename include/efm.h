@@ -126,6 +126,17 @@ EFM_API int64_t efm_workspace_bytes(const efm_ctx *ctx, int save_borders);
 EFM_API int efm_forward(efm_ctx *ctx, float *gathers_dev, int save, void *stream);
 
 /*
+ * efm_forward that also sums the forward illumination of every instance: after each
+ * velocity update illum[cell] += vx^2 + vy^2 + vz^2.  No counterpart in the reference (an
+ * input of the learned preconditioner, standing in for the pseudo-Hessian diagonal).
+ * illum_dev: one [ny][nz][nx] volume per instance, concatenated in id order (the same
+ * per-instance offsets as the g_lambda part of efm_gradient's buffer divided by three, i.e.
+ * the sum of the earlier instances' cells); the sums add to its contents, so zero it first.
+ */
+EFM_API int efm_forward_illumination(efm_ctx *ctx, float *gathers_dev, int save, float *illum_dev,
+                                     void *stream);
+
+/*
  * Adjoint pass (Elastic3D.backwardFields_FowardFieldsRemake, :1929-2054, and
  * Elastic3D.backwardFields, :2056-2082): adjoint propagation with the residual injected
  * into the velocities (kernel_add_adjoint_source, :310-322).

@@ -274,10 +274,12 @@ def cpml_zone_mask(ny, nz, nx, width):
 
 # --------------------------------------------------------------------------- solves
 def forward(lam, mu, rho, cp, wavelet, dt, dx, src, mt, rec, save_borders=False,
-            return_state=False):
+            return_state=False, illumination=False):
     """Elastic3D.forwardFields (:1812-1847), per step: tau update, source, v update,
     receivers, (border strips).  Returns gathers (3, nt, nrec) float64 and optionally
-    the saved strips (nt, 3, nstrip) and the final state."""
+    the saved strips (nt, 3, nstrip), the final state and the illumination
+    sum_t (vx^2 + vy^2 + vz^2) after each velocity update (no counterpart in the reference;
+    checks efm_forward_illumination)."""
     md = Model(lam, mu, rho)
     ny, nz, nx = md.lam.shape
     st = State(ny, nz, nx)
@@ -287,6 +289,7 @@ def forward(lam, mu, rho, cp, wavelet, dt, dx, src, mt, rec, save_borders=False,
     width = _cpml_width(cp, nx)
     bmask = border_mask(ny, nz, nx, width) if save_borders else None
     borders = [] if save_borders else None
+    illum = np.zeros((ny, nz, nx)) if illumination else None
     for it in range(nt):
         stress_step(st, md, cp, dt, dx)
         add_source(st, src, mt, wavelet[it])
@@ -294,11 +297,15 @@ def forward(lam, mu, rho, cp, wavelet, dt, dx, src, mt, rec, save_borders=False,
         g[0, it], g[1, it], g[2, it] = record(st, rec)
         if save_borders:
             borders.append(np.stack([st.vx[bmask], st.vy[bmask], st.vz[bmask]]))
+        if illumination:
+            illum += st.vx ** 2 + st.vy ** 2 + st.vz ** 2
     out = [g]
     if save_borders:
         out.append(np.stack(borders))
     if return_state:
         out.append(st)
+    if illumination:
+        out.append(illum)
     return out[0] if len(out) == 1 else tuple(out)
 
 

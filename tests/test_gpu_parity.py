@@ -371,3 +371,31 @@ def test_graph_replay_equals_step_launches(golden_c1scale, cuda):
     for a, c in zip(out[1], out[0]):
         assert np.array_equal(np.asarray(a), np.asarray(c))
     assert out[1][3][0] == int(d["nt"])  # EFM_K_FWD_STRESS: one launch per step
+
+
+@pytest.mark.parametrize("stream", [1, 0])
+def test_forward_illumination_matches_oracle(golden_c1scale, cuda, stream):
+    """efm_forward_illumination: sum_t |v|^2 against the FP64 oracle (1e-4, FP32 sums over 300
+    steps), on the streaming and the one-thread-per-cell kernels; the gathers are the same
+    as efm_forward's, and a second call adds the same sums again."""
+    import torch
+
+    import efm_oracle as O
+    from elastic_fm_vp_vs_rho_b200 import _lib
+    d = golden_c1scale
+    b = _batch(d, d["lam_true"], d["mu_true"], d["rho_true"], d["mt_obs"])
+    b.set_option(_lib.EFM_OPT_STREAM_KERNELS, stream)
+    ill = torch.zeros(b.illum_size, dtype=torch.float32, device="cuda")
+    g1 = b.forward(illum=ill).clone()
+    g0 = b.forward()
+    b.status()
+    assert torch.equal(g0, g1)
+    one = b.illum_view(ill, 0).cpu().numpy().copy()
+    b.forward(illum=ill)
+    b.status()
+    assert rel_err(b.illum_view(ill, 0).cpu().numpy(), 2 * one) < 1e-6
+    rec = _rec(d)
+    _, ref = O.forward(d["lam_true"], d["mu_true"], d["rho_true"], _cp(d), d["waveform"],
+                       float(d["dt"]), float(d["dx"]), tuple(d["src"][0]), d["mt_obs"],
+                       (rec[:, 0], rec[:, 1], rec[:, 2]), illumination=True)
+    assert rel_err(one, ref) < 1e-4

@@ -121,6 +121,10 @@ def test_network_state_and_adam_on_cpu():
     f = features(g3, p3)
     assert f.shape == (2, 3, 4, 16) and f.dtype == torch.bfloat16
     assert float(f[..., :3].float().abs().max()) <= 1.0
+    assert float(f[..., 7].float().abs().max()) == 0.0  # no illumination given
+    ill = torch.rand(2, 3, 4) * 1e-12 + 1e-16
+    v = features(g3, p3, ill)[..., 7].float()
+    assert float(v.min()) >= 0.0 and float(v.max()) == 1.0  # log-compressed, max -> 1
     out = torch.zeros(2, 3, 4, 16)
     loss, d = mse_grad(out, torch.ones(2, 3, 4, 3))
     assert abs(loss - 1.0) < 1e-12 and float(d[..., 3:].abs().max()) == 0.0

@@ -649,8 +649,9 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
             }
         } else {
             // forward / adjoint: the plane's update, with or without the memory-variable code
-            auto plane = [&](auto tag) -> bool {
+            auto plane = [&](auto tag, auto rtag) -> bool {
                 constexpr bool PML = decltype(tag)::value;
+                constexpr bool REC = decltype(rtag)::value;  // this plane of the tile has receivers
                 PsiPlane P{0, 0, 0, false};
                 float pp[ROWS][9];
                 if (PML) {
@@ -673,7 +674,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     const int z = T.z0 + lr + 4 * h;
                     const bool guard = plane_in && rw[h].in;
                     bool more = false;  // the cell may hold several receivers
-                    const int rq = rec_plane && colgrid[h] ? efm_rec_first(I, x, y, z, &more) : -1;
+                    const int rq = REC && colgrid[h] ? efm_rec_first(I, x, y, z, &more) : -1;
                     const bool rec = rq >= 0;
                     if (!(guard || rec)) continue;
                     const int hi = rw[h].hidx, ci = rw[h].cidx;
@@ -778,7 +779,12 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
             bool wpml = ypml;  // warp-uniform: some lane of this warp has memory variables here
 #pragma unroll
             for (int h = 0; h < ROWS; ++h) wpml = wpml || rw[h].wx || rw[h].wz;
-            mine = wpml ? plane(Tag<true>{}) : plane(Tag<false>{});
+            // four instantiations: the receiver code only runs on the few planes that hold
+            // receivers of this tile (block-uniform), the CPML code in the warps that need it
+            if (rec_plane)
+                mine = wpml ? plane(Tag<true>{}, Tag<true>{}) : plane(Tag<false>{}, Tag<true>{});
+            else
+                mine = wpml ? plane(Tag<true>{}, Tag<false>{}) : plane(Tag<false>{}, Tag<false>{});
         }
         ok = __syncthreads_and(mine) != 0;
         if (!ok) break;

@@ -132,6 +132,7 @@ EFM_API int efm_forward(efm_ctx *ctx, float *gathers_dev, int save, void *stream
  * illum_dev: one [ny][nz][nx] volume per instance, concatenated in id order (the same
  * per-instance offsets as the g_lambda part of efm_gradient's buffer divided by three, i.e.
  * the sum of the earlier instances' cells); the sums add to its contents, so zero it first.
+ * A null illum_dev makes it efm_forward.
  */
 EFM_API int efm_forward_illumination(efm_ctx *ctx, float *gathers_dev, int save, float *illum_dev,
                                      void *stream);

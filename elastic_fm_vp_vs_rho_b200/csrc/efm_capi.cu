@@ -75,6 +75,7 @@ struct Inst {
     // exact adjoint: checkpoints of (v, tau, psi), a segment of per-step (v, tau), and the
     // adjoint memory variables (two sets, read / written alternately)
     float *ckpt = nullptr, *segbuf = nullptr, *apsi = nullptr;
+    float *exscr = nullptr;  // exact adjoint: 12 scratch volumes of the per-cell passes + 6 averages
     int ck_every = 0, nck = 0;
     bool ck_saved = false;
     int64_t ncell = 0, strip_n = 0, psx_n = 0, psy_n = 0, psz_n = 0;
@@ -399,7 +400,8 @@ void free_inst(Inst &I) {
     cudaFree(I.ckpt);
     cudaFree(I.segbuf);
     cudaFree(I.apsi);
-    I.ckpt = I.segbuf = I.apsi = nullptr;
+    cudaFree(I.exscr);
+    I.ckpt = I.segbuf = I.apsi = I.exscr = nullptr;
     I.ck_every = I.nck = 0;
     I.cpml = nullptr;
     I.rec_mask = nullptr;
@@ -572,13 +574,15 @@ int ensure_exact(efm_ctx *ctx) {
         cudaFree(I.ckpt);
         cudaFree(I.segbuf);
         cudaFree(I.apsi);
-        I.ckpt = I.segbuf = I.apsi = nullptr;
+        cudaFree(I.exscr);
+        I.ckpt = I.segbuf = I.apsi = I.exscr = nullptr;
         I.ck_every = K;
         I.nck = (I.nt + K - 1) / K;
         const size_t nck = (size_t)std::max(1, I.nck - 1);
         if (cudaMalloc(&I.ckpt, nck * ckpt_floats(I) * sizeof(float)) != cudaSuccess ||
             cudaMalloc(&I.segbuf, (size_t)(K + 1) * 9 * I.ncell * sizeof(float)) != cudaSuccess ||
-            cudaMalloc(&I.apsi, 2 * psi_floats(I) * sizeof(float)) != cudaSuccess) {
+            cudaMalloc(&I.apsi, 2 * psi_floats(I) * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&I.exscr, 18 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
             cudaGetLastError();
             return fail(EFM_ERR_NOMEM, "cannot allocate exact-adjoint checkpoints (interval " +
                                            std::to_string(K) + ")");
@@ -700,6 +704,8 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
         Inst &I = ctx->inst[i];
         EFM_CK(cudaMemsetAsync(I.bv(0), 0, 9 * I.ncell * sizeof(float), s));
         EFM_CK(cudaMemsetAsync(I.apsi, 0, 2 * psi_floats(I) * sizeof(float), s));
+        // cells outside the update domain read zero from the scratch of the per-cell passes
+        EFM_CK(cudaMemsetAsync(I.exscr, 0, 18 * (size_t)I.ncell * sizeof(float), s));
         EFM_CK(cudaMemsetAsync(grad + I.grad_off, 0, 3 * I.ncell * sizeof(float), s));
         if (mt) EFM_CK(cudaMemsetAsync(mtg + (size_t)i * EFM_NSRC * 6, 0, EFM_NSRC * 6 * sizeof(double), s));
         EfmExact e;
@@ -729,6 +735,8 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
         e.g_lam = grad + I.grad_off;
         e.g_mu = grad + I.grad_off + I.ncell;
         e.g_rho = grad + I.grad_off + 2 * I.ncell;
+        e.scr = I.exscr;
+        e.avg = I.exscr + 12 * I.ncell;
         e.nsrc = I.nsrc;
         for (int q = 0; q < EFM_NSRC; ++q) {
             e.sx[q] = I.src[q][0];
@@ -752,6 +760,11 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
     }
     EFM_CK(cudaMemcpyAsync(ctx->d_ex, tab.data(), tab.size() * sizeof(EfmExact),
                            cudaMemcpyHostToDevice, s));
+    // the model's harmonic averages, once per call
+    if ((rc = timed_launch(ctx, EFM_K_MODEL_AUX, s, [&] {
+             return efm_launch_exact(3, ctx->d_ex, n, tiles, 0, 0, s);
+         })))
+        return rc;
     bool st = false;
     if ((rc = prepare_forward(ctx, nullptr, false, true, s, &st))) return rc;
     const int K = ctx->inst[0].ck_every;

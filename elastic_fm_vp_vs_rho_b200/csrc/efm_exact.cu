@@ -5,7 +5,7 @@
 // images with zero-lag correlations: a descent direction, not dJ/dm.  This file is the
 // transpose of each half-step of kernel_Tau (:59-128) and kernel_Vx_Vy_Vz (:133-188),
 // including the CPML memory-variable recursions psi = b psi + a d, written as gathers (no
-// atomics).  Per step n, backwards:
+// atomics; each half-step as a per-cell pass and a gather pass).  Per step n, backwards:
 //   inject      vbar(rec) += res[n]
 //   velocity^T  ubar_k = k B_i vbar_i ; gbar_k = (1 + a_k) ubar_k + a_k psibar_k
 //               taubar += D_T^T gbar ; psibar_k <- b_k (psibar_k + ubar_k)
@@ -64,18 +64,26 @@ struct G {
         const int64_t i = psi_idx(d, v, x, y, z);
         return i < 0 ? 0.f : I.pin[i];
     }
-    __device__ float buoy_avg(int comp, int x, int y, int z) const {
+    // harmonic 2-point buoyancy of velocity component comp (:153-159), from rho
+    __device__ float buoy_avg_of(int comp, int x, int y, int z) const {
         const int64_t c = lin(x, y, z);
         const int64_t e = comp == 0 ? 1 : (comp == 1 ? SY : SZ);
         const float b0 = 1.f / I.rho[c], b1 = 1.f / I.rho[c + e];
         return 2.f * b0 * b1 / (b0 + b1);
     }
-    __device__ float mu_avg(int pair, int x, int y, int z) const {
-        // pair 0: xy, 1: xz, 2: yz (harmonic 4-point, :87-89)
+    // harmonic 4-point mu, pair 0: xy, 1: xz, 2: yz (:87-89), from mu
+    __device__ float mu_avg_of(int pair, int x, int y, int z) const {
         const int64_t c = lin(x, y, z);
         const int64_t e1 = pair == 2 ? SY : 1, e2 = pair == 0 ? SY : SZ;
         const float *m = I.mu;
         return 1.f / (0.25f / m[c] + 0.25f / m[c + e1] + 0.25f / m[c + e2] + 0.25f / m[c + e1 + e2]);
+    }
+    // the same, precomputed once per gradient call for the cells of the update domain
+    __device__ float buoy_avg(int comp, int x, int y, int z) const {
+        return I.avg[(3 + comp) * (I.slot_stride / 9) + lin(x, y, z)];
+    }
+    __device__ float mu_avg(int pair, int x, int y, int z) const {
+        return I.avg[pair * (I.slot_stride / 9) + lin(x, y, z)];
     }
 };
 
@@ -89,15 +97,6 @@ __device__ __forceinline__ int vt_comp(int k) {
     return c[k];
 }
 
-__device__ float gbar(const G &g, int kk, int x, int y, int z) {
-    if (!g.in(x, y, z)) return 0.f;
-    const int i = vt_comp(kk), d = vt_family(kk);
-    const float ub = g.I.k * g.buoy_avg(i, x, y, z) * g.I.bv[i][g.lin(x, y, z)];
-    const int q = d == 0 ? x : (d == 1 ? y : z);
-    const float a = g.a(d, q);
-    if (a == 0.f) return ub;
-    return (1.f + a) * ub + a * g.psi_in(d, 3 + kk % 3, x, y, z);
-}
 
 // ---- stress transpose helpers: the 9 stress-update differences
 // k: 0 vx_x 1 vy_x 2 vz_x (family x vars 0,1,2) | 3 vy_y 4 vx_y 5 vz_y (y) |
@@ -124,16 +123,6 @@ __device__ void ebar_all(const G &g, int x, int y, int z, float e[9]) {
     e[8] = syz;  // vy_z (tau_yz)
 }
 
-__device__ float dbar(const G &g, int kk, int x, int y, int z) {
-    if (!g.in(x, y, z)) return 0.f;
-    float e[9];
-    ebar_all(g, x, y, z, e);
-    const int d = kk / 3;
-    const int q = d == 0 ? x : (d == 1 ? y : z);
-    const float a = g.a(d, q);
-    if (a == 0.f) return e[kk];
-    return (1.f + a) * e[kk] + a * g.psi_in(d, kk % 3, x, y, z);
-}
 
 __device__ __forceinline__ const EfmExact &find(const EfmExact *t, int n, int b) {
     int lo = 0, hi = n - 1;
@@ -172,36 +161,54 @@ efm_exact_inject(const EfmExact *__restrict__ t, int n, int step) {
     }
 }
 
+// Each transposed half-step runs as two launches: the first computes, once per cell, the
+// quantities its neighbours gather (gbar / dbar for the 9 differences, and the three shear
+// products of the mu gradient) into the instance's scratch volumes; the second gathers them.
+// A single gather kernel would recompute them for every neighbour (15-18 times per cell).
+// Scratch entries of cells outside the update domain are never written and stay zero (the
+// host clears the scratch before the pass), which is the zero the gathers need there.
+
+// The model's harmonic averages at every cell of the update domain (the model is fixed
+// during a gradient call; every pass reads them instead of recomputing them per neighbour).
 __global__ void __launch_bounds__(EFM_THREADS)
-efm_exact_velocity_T(const EfmExact *__restrict__ t, int n, int step, int slot) {
+efm_exact_averages(const EfmExact *__restrict__ t, int n) {
+    const EfmExact &I = find(t, n, blockIdx.x);
+    int x, y, z;
+    if (!cell_of(I, x, y, z)) return;
+    G g(I);
+    if (!g.in(x, y, z)) return;
+    const int64_t p = g.lin(x, y, z), N = I.slot_stride / 9;
+    float *avg = const_cast<float *>(I.avg);
+    for (int q = 0; q < 3; ++q) {
+        avg[q * N + p] = g.mu_avg_of(q, x, y, z);
+        avg[(3 + q) * N + p] = g.buoy_avg_of(q, x, y, z);
+    }
+}
+
+__global__ void __launch_bounds__(EFM_THREADS)
+efm_exact_velocity_T_cells(const EfmExact *__restrict__ t, int n, int step, int slot) {
     const EfmExact &I = find(t, n, blockIdx.x);
     int x, y, z;
     if (!cell_of(I, x, y, z)) return;
     G g(I);
     const int64_t p = g.lin(x, y, z);
+    const int64_t N = I.slot_stride / 9;
     if (g.in(x, y, z)) {
-        // taubar += D_T^T gbar (gather)
-        I.bt[0][p] += gbar(g, 0, x - 1, y, z) - gbar(g, 0, x, y, z);
-        I.bt[1][p] += gbar(g, 3, x, y - 1, z) - gbar(g, 3, x, y, z);
-        I.bt[2][p] += gbar(g, 6, x, y, z - 1) - gbar(g, 6, x, y, z);
-        I.bt[3][p] += gbar(g, 4, x, y, z) - gbar(g, 4, x, y + 1, z) + gbar(g, 1, x, y, z) - gbar(g, 1, x + 1, y, z);
-        I.bt[4][p] += gbar(g, 7, x, y, z) - gbar(g, 7, x, y, z + 1) + gbar(g, 2, x, y, z) - gbar(g, 2, x + 1, y, z);
-        I.bt[5][p] += gbar(g, 8, x, y, z) - gbar(g, 8, x, y, z + 1) + gbar(g, 5, x, y, z) - gbar(g, 5, x, y + 1, z);
-        // memory variables of the velocity update: psibar <- b (psibar + ubar)
+        float ub[3];
+        for (int i = 0; i < 3; ++i) ub[i] = I.k * g.buoy_avg(i, x, y, z) * I.bv[i][p];
         for (int kk = 0; kk < 9; ++kk) {
-            const int d = kk / 3;
-            const int64_t ix = g.psi_idx(d, 3 + kk % 3, x, y, z);
-            if (ix < 0) continue;
+            const int i = vt_comp(kk), d = vt_family(kk);
             const int q = d == 0 ? x : (d == 1 ? y : z);
-            const int i = vt_comp(kk);
-            const float ub = I.k * g.buoy_avg(i, x, y, z) * I.bv[i][p];
-            I.pout[ix] = g.b(d, q) * (I.pin[ix] + ub);
+            const float a = g.a(d, q);
+            I.scr[kk * N + p] = a == 0.f ? ub[i] : (1.f + a) * ub[i] + a * g.psi_in(d, 3 + kk % 3, x, y, z);
+            // memory variables of the velocity update: psibar <- b (psibar + ubar)
+            const int64_t ix = g.psi_idx(d, 3 + kk % 3, x, y, z);
+            if (ix >= 0) I.pout[ix] = g.b(d, q) * (I.pin[ix] + ub[i]);
         }
     }
     // rho gradient: -1/2 sum_i B_i(c) vbar_i(c) dv_i(c) over c in {p, p - e_i} that are updated
     const float *vn = I.seg + (int64_t)slot * I.slot_stride;
     const float *vm = vn - I.slot_stride;
-    const int64_t N = I.slot_stride / 9;
     float acc = 0.f;
     const int64_t e[3] = {1, g.SY, g.SZ};
     const int dx_[3] = {1, 0, 0}, dy_[3] = {0, 1, 0}, dz_[3] = {0, 0, 1};
@@ -218,81 +225,117 @@ efm_exact_velocity_T(const EfmExact *__restrict__ t, int n, int step, int slot) 
 }
 
 __global__ void __launch_bounds__(EFM_THREADS)
-efm_exact_stress_T(const EfmExact *__restrict__ t, int n, int step, int slot) {
+efm_exact_velocity_T_gather(const EfmExact *__restrict__ t, int n, int step, int slot) {
+    const EfmExact &I = find(t, n, blockIdx.x);
+    int x, y, z;
+    if (!cell_of(I, x, y, z)) return;
+    G g(I);
+    if (!g.in(x, y, z)) return;
+    const int64_t p = g.lin(x, y, z);
+    const int64_t N = I.slot_stride / 9;
+    const float *S = I.scr;
+    auto gb = [&](int kk, int64_t c) { return S[kk * N + c]; };
+    const int64_t X = 1, Y = g.SY, Z = g.SZ;
+    // taubar += D_T^T gbar (gather)
+    I.bt[0][p] += gb(0, p - X) - gb(0, p);
+    I.bt[1][p] += gb(3, p - Y) - gb(3, p);
+    I.bt[2][p] += gb(6, p - Z) - gb(6, p);
+    I.bt[3][p] += gb(4, p) - gb(4, p + Y) + gb(1, p) - gb(1, p + X);
+    I.bt[4][p] += gb(7, p) - gb(7, p + Z) + gb(2, p) - gb(2, p + X);
+    I.bt[5][p] += gb(8, p) - gb(8, p + Z) + gb(5, p) - gb(5, p + Y);
+}
+
+__global__ void __launch_bounds__(EFM_THREADS)
+efm_exact_stress_T_cells(const EfmExact *__restrict__ t, int n, int step, int slot) {
+    const EfmExact &I = find(t, n, blockIdx.x);
+    int x, y, z;
+    if (!cell_of(I, x, y, z)) return;
+    G g(I);
+    if (!g.in(x, y, z)) return;
+    const int64_t p = g.lin(x, y, z);
+    const float *tn = I.seg + (int64_t)slot * I.slot_stride + 3 * (I.slot_stride / 9);
+    const float *tm = tn - I.slot_stride;
+    const int64_t N = I.slot_stride / 9;
+    // stress increment of step n at this cell, without the source
+    auto dtau = [&](int comp) {
+        float d = tn[comp * N + p] - tm[comp * N + p];
+        for (int s = 0; s < I.nsrc; ++s)
+            if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s]) d -= I.mt[s][comp] * I.wav[step];
+        return d;
+    };
+    // MT gradient at the source cell: Mbar += w[n] taubar(src)
+    if (I.mtg != nullptr)
+        for (int s = 0; s < I.nsrc; ++s)
+            if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s])
+                for (int c6 = 0; c6 < 6; ++c6)
+                    I.mtg[6 * s + c6] += (double)I.wav[step] * (double)I.bt[c6][p];
+    float e[9];
+    ebar_all(g, x, y, z, e);
+    for (int kk = 0; kk < 9; ++kk) {
+        const int d = kk / 3;
+        const int q = d == 0 ? x : (d == 1 ? y : z);
+        const float a = g.a(d, q);
+        I.scr[kk * N + p] = a == 0.f ? e[kk] : (1.f + a) * e[kk] + a * g.psi_in(d, kk % 3, x, y, z);
+        const int64_t ix = g.psi_idx(d, kk % 3, x, y, z);
+        if (ix >= 0) I.pout[ix] = g.b(d, q) * (I.pin[ix] + e[kk]);
+    }
+    // lambda and diagonal mu terms
+    const float lam = I.lam[p], mu = I.mu[p];
+    const float b0 = I.bt[0][p], b1 = I.bt[1][p], b2 = I.bt[2][p];
+    const float d0 = dtau(0), d1 = dtau(1), d2 = dtau(2);
+    const float sb = b0 + b1 + b2, sd = d0 + d1 + d2;
+    const float inv = 1.f / (3.f * lam + 2.f * mu);
+    I.g_lam[p] += sb * sd * inv;
+    I.g_mu[p] += (b0 * d0 + b1 * d1 + b2 * d2 - lam * sb * sd * inv) / mu;
+    // shear products taubar_ij * dtau_ij * mu_ij of this cell, gathered by the mu(p) of the
+    // four cells whose harmonic averages it enters
+    for (int pair = 0; pair < 3; ++pair)
+        I.scr[(9 + pair) * N + p] = I.bt[3 + pair][p] * dtau(3 + pair) * g.mu_avg(pair, x, y, z);
+}
+
+__global__ void __launch_bounds__(EFM_THREADS)
+efm_exact_stress_T_gather(const EfmExact *__restrict__ t, int n, int step, int slot) {
     const EfmExact &I = find(t, n, blockIdx.x);
     int x, y, z;
     if (!cell_of(I, x, y, z)) return;
     G g(I);
     const int64_t p = g.lin(x, y, z);
-    const float *tn = I.seg + (int64_t)slot * I.slot_stride + 3 * (I.slot_stride / 9);
-    const float *tm = tn - I.slot_stride;
     const int64_t N = I.slot_stride / 9;
-    // stress increment of step n at a cell, without the source
-    auto dtau = [&](int comp, int cx, int cy, int cz) {
-        const int64_t c = g.lin(cx, cy, cz);
-        float d = tn[comp * N + c] - tm[comp * N + c];
-        for (int s = 0; s < I.nsrc; ++s)
-            if (cx == I.sx[s] && cy == I.sy[s] && cz == I.sz[s]) d -= I.mt[s][comp] * I.wav[step];
-        return d;
-    };
+    const float *S = I.scr;
+    auto db = [&](int kk, int64_t c) { return S[kk * N + c]; };
+    const int64_t X = 1, Y = g.SY, Z = g.SZ;
     if (g.in(x, y, z)) {
-        // MT gradient at the source cell: Mbar += w[n] taubar(src)
-        if (I.mtg != nullptr)
-            for (int s = 0; s < I.nsrc; ++s)
-                if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s])
-                    for (int c6 = 0; c6 < 6; ++c6)
-                        I.mtg[6 * s + c6] += (double)I.wav[step] * (double)I.bt[c6][p];
         // vbar += D_V^T dbar (gather)
-        I.bv[0][p] += dbar(g, 0, x, y, z) - dbar(g, 0, x + 1, y, z) + dbar(g, 7, x, y, z - 1) - dbar(g, 7, x, y, z) +
-                      dbar(g, 4, x, y - 1, z) - dbar(g, 4, x, y, z);
-        I.bv[1][p] += dbar(g, 3, x, y, z) - dbar(g, 3, x, y + 1, z) + dbar(g, 1, x - 1, y, z) - dbar(g, 1, x, y, z) +
-                      dbar(g, 8, x, y, z - 1) - dbar(g, 8, x, y, z);
-        I.bv[2][p] += dbar(g, 6, x, y, z) - dbar(g, 6, x, y, z + 1) + dbar(g, 2, x - 1, y, z) - dbar(g, 2, x, y, z) +
-                      dbar(g, 5, x, y - 1, z) - dbar(g, 5, x, y, z);
-        float e[9];
-        ebar_all(g, x, y, z, e);
-        for (int kk = 0; kk < 9; ++kk) {
-            const int d = kk / 3;
-            const int64_t ix = g.psi_idx(d, kk % 3, x, y, z);
-            if (ix < 0) continue;
-            const int q = d == 0 ? x : (d == 1 ? y : z);
-            I.pout[ix] = g.b(d, q) * (I.pin[ix] + e[kk]);
-        }
-        // lambda and diagonal mu terms at p
-        const float lam = I.lam[p], mu = I.mu[p];
-        const float b0 = I.bt[0][p], b1 = I.bt[1][p], b2 = I.bt[2][p];
-        const float d0 = dtau(0, x, y, z), d1 = dtau(1, x, y, z), d2 = dtau(2, x, y, z);
-        const float sb = b0 + b1 + b2, sd = d0 + d1 + d2;
-        const float inv = 1.f / (3.f * lam + 2.f * mu);
-        I.g_lam[p] += sb * sd * inv;
-        I.g_mu[p] += (b0 * d0 + b1 * d1 + b2 * d2 - lam * sb * sd * inv) / mu;
+        I.bv[0][p] += db(0, p) - db(0, p + X) + db(7, p - Z) - db(7, p) + db(4, p - Y) - db(4, p);
+        I.bv[1][p] += db(3, p) - db(3, p + Y) + db(1, p - X) - db(1, p) + db(8, p - Z) - db(8, p);
+        I.bv[2][p] += db(6, p) - db(6, p + Z) + db(2, p - X) - db(2, p) + db(5, p - Y) - db(5, p);
     }
     // shear mu terms: mu(p) enters mu_xy, mu_xz, mu_yz of up to four updated cells each
-    float acc = 0.f;
     const float mup = I.mu[p];
     const float f = 0.25f / (mup * mup);
+    float acc = 0.f;
     for (int pair = 0; pair < 3; ++pair) {
-        const int comp = 3 + pair;  // txy, txz, tyz
-        const int ax1 = pair == 2 ? 1 : 0;  // first axis: x for xy/xz, y for yz
-        const int ax2 = pair == 0 ? 1 : 2;  // second axis: y for xy, z for xz/yz
-        for (int s1 = 0; s1 < 2; ++s1)
-            for (int s2 = 0; s2 < 2; ++s2) {
-                int cx = x, cy = y, cz = z;
-                if (ax1 == 0) cx -= s1; else cy -= s1;
-                if (ax2 == 1) cy -= s2; else cz -= s2;
-                if (!g.in(cx, cy, cz)) continue;
-                const float m4 = g.mu_avg(pair, cx, cy, cz);
-                acc += I.bt[comp][g.lin(cx, cy, cz)] * dtau(comp, cx, cy, cz) * m4 * f;
-            }
+        const int64_t e1 = pair == 2 ? Y : X;  // first axis: x for xy/xz, y for yz
+        const int64_t e2 = pair == 0 ? Y : Z;  // second axis: y for xy, z for xz/yz
+        const float *T = S + (9 + pair) * N;
+        acc += T[p] + T[p - e1] + T[p - e2] + T[p - e1 - e2];
     }
-    I.g_mu[p] += acc;
+    I.g_mu[p] += acc * f;
 }
 
 extern "C" cudaError_t efm_launch_exact(int kind, const EfmExact *t, int n, int tiles, int step,
                                         int slot, cudaStream_t s) {
-    if (kind == 0) efm_exact_inject<<<n, EFM_THREADS, 0, s>>>(t, n, step);
-    else if (kind == 1) efm_exact_velocity_T<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
-    else efm_exact_stress_T<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
+    if (kind == 3) {
+        efm_exact_averages<<<tiles, EFM_THREADS, 0, s>>>(t, n);
+    } else if (kind == 0) {
+        efm_exact_inject<<<n, EFM_THREADS, 0, s>>>(t, n, step);
+    } else if (kind == 1) {
+        efm_exact_velocity_T_cells<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
+        efm_exact_velocity_T_gather<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
+    } else {
+        efm_exact_stress_T_cells<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
+        efm_exact_stress_T_gather<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
+    }
     return cudaGetLastError();
 }
 

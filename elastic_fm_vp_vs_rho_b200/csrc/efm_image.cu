@@ -110,9 +110,13 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     const int clast = ye - 1;  // cell planes ys .. ye-1
     int h_hi = min(hlast, R.p0 + IMG_RH - 1);
     int c_hi = min(clast, R.c0 + IMG_RC - 1);
+    // two issuing threads in different warps: the halo ring's loads and the cell ring's
+    // (separate barriers) go out in parallel
     if (threadIdx.x == 0) {
-        for (int q = 0; q < IMG_NH + IMG_NC; ++q) efm_prefetch_tmap(tm + q);
+        for (int q = 0; q < IMG_NH; ++q) efm_prefetch_tmap(tm + q);
         for (int p = R.p0; p <= h_hi; ++p) issue_halo(R, tm, x0, z0, p);
+    } else if (threadIdx.x == 32) {
+        for (int q = IMG_NH; q < IMG_NH + IMG_NC; ++q) efm_prefetch_tmap(tm + q);
         for (int p = R.c0; p <= c_hi; ++p) issue_cell(R, tm, x0, z0, p);
     }
     const int hidx = (lz + 2) * EFM_HX + lx + EFM_HX_OFF;
@@ -175,6 +179,7 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         if (!ok) break;
         if (threadIdx.x == 0) {
             if (j - 2 + IMG_RH <= hlast) issue_halo(R, tm, x0, z0, j - 2 + IMG_RH);
+        } else if (threadIdx.x == 32) {
             if (j + IMG_RC <= clast) issue_cell(R, tm, x0, z0, j + IMG_RC);
         }
         if (j - 2 + IMG_RH <= hlast) h_hi = j - 2 + IMG_RH;

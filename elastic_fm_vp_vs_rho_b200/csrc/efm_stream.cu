@@ -78,7 +78,7 @@ __device__ __forceinline__ void issue_plane(const Ring<ROWS, SR> &R, const CUten
         efm_tma_load_3d(st + NH * HB + f * CB, tm + NH + f, bar, x0, z0, p);
 }
 
-// End of plane j, thread 0, after the block barrier: store the n updated cell fields
+// End of plane j, issuing thread, after the block barrier: store the n updated cell fields
 // [f0, f0 + n) of plane j's stage through the maps sm[0 .. n) (when `store`), close plane j's
 // bulk group, and refill the stage of plane j-1 with plane j-1+SR once the store out of it
 // (closed one plane earlier) has finished reading it.
@@ -121,11 +121,22 @@ __device__ void drain(const Ring<ROWS, SR> &R, int first, int last) {
     for (int p = first; p <= last; ++p) efm_mbar_wait(&R.bar[R.stage(p)], R.parity(p), nullptr);
 }
 
+// The thread that issues the block's TMA loads and stores: lane 0 of a warp of the first
+// thread row whose 32 cells of x hold no x-CPML cell, when there is one.  Such a warp
+// finishes each plane before the CPML warps, so the issue work stays off the slowest warp.
+__device__ __forceinline__ int stream_issuer(const Tile &T, int nx, int W) {
+    for (int half = 1; half >= 0; --half) {
+        const int xa = T.x0 + 32 * half;
+        if (xa >= W && xa + 31 < nx - W) return 32 * half;
+    }
+    return 0;
+}
+
 // Block set-up shared by both kernels: barriers, prologue loads, source flag, receiver bits.
 template <int ROWS, int SR, int NH, int NC>
 __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ring<ROWS, SR> &R,
                                              const CUtensorMap *tm, int *s_flags,
-                                             unsigned long long *s_recbits) {
+                                             unsigned long long *s_recbits, int iss) {
     if (threadIdx.x == 0) {
         for (int s = 0; s < SR; ++s) efm_mbar_init(&R.bar[s], 1);
         efm_fence_barrier_init();
@@ -157,7 +168,7 @@ __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ri
     // preceding kernel has finished
     efm_pdl_wait();
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if ((int)threadIdx.x == iss) {
         for (int q = 0; q < NH + NC; ++q) efm_prefetch_tmap(tm + q);
         for (int p = R.p0; p <= min(T.ye, R.p0 + SR - 1); ++p)
             issue_plane<ROWS, SR, NH, NC>(R, tm, T.x0, T.z0, p);
@@ -426,7 +437,8 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
-    stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    const int iss = stream_issuer(T, nx, W);
+    stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const bool has_src = s_src != 0;
     const Hot H = make_hot(I, 0);
     Row rw[ROWS];
@@ -498,11 +510,11 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
         const bool mine = wpml ? plane(Tag<true>{}) : plane(Tag<false>{});
         ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
         if (!ok) break;
-        if (threadIdx.x == 0)
+        if ((int)threadIdx.x == iss)
             advance<ROWS, SR, NH, NC>(R, tm, tm + NH + 1, 1, 6, plane_in, T.x0, T.z0, j, last);
         if (j - 1 + SR <= last) issued_hi = j - 1 + SR;
     }
-    if (threadIdx.x == 0) efm_bulk_wait_all();
+    if ((int)threadIdx.x == iss) efm_bulk_wait_all();
     if (!ok) drain(R, R.p0, issued_hi);  // no load may still target this block's smem
 }
 
@@ -525,7 +537,8 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
-    stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec);
+    const int iss = stream_issuer(T, nx, W);
+    stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const unsigned long long recbits = s_rec;
     const Hot H = make_hot(I, 1);
     float *const border = I.border;
@@ -788,10 +801,11 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
         }
         ok = __syncthreads_and(mine) != 0;
         if (!ok) break;
-        if (threadIdx.x == 0) advance<ROWS, SR, NH, NC>(R, tm, stm, 1, 3, store, T.x0, T.z0, j, last);
+        if ((int)threadIdx.x == iss)
+            advance<ROWS, SR, NH, NC>(R, tm, stm, 1, 3, store, T.x0, T.z0, j, last);
         if (j - 1 + SR <= last) issued_hi = j - 1 + SR;
     }
-    if (threadIdx.x == 0) efm_bulk_wait_all();
+    if ((int)threadIdx.x == iss) efm_bulk_wait_all();
     if (!ok) drain(R, R.p0, issued_hi);
 }
 

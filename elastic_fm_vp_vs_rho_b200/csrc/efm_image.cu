@@ -122,7 +122,11 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     const int hidx = (lz + 2) * EFM_HX + lx + EFM_HX_OFF;
     const int cidx = lz * EFM_STX + lx;
     const bool colin = x >= EFM_HS && x < nx - EFM_HS && z >= EFM_HS && z < nz - EFM_HS;
-    const int64_t SZ = nx, SY = (int64_t)nx * nz;
+    const int64_t SY = (int64_t)nx * nz;
+    // gradient volumes and this thread's cell offset inside a plane, read once (the waits'
+    // memory clobbers would otherwise reload the table fields every plane)
+    float *const g_lam = I.g_lam, *const g_mu = I.g_mu, *const g_rho = I.g_rho;
+    const int cxz = x + nx * z;
     const float idt = I.inv_dt, idx = I.inv_dx;
     bool ok;
     {
@@ -170,10 +174,10 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
                               f * (lpm2 * btzz - lam * btxx - lam * btyy) * ez +
                               imu_xy * btxy * (eyx + exy) + imu_xz * btxz * (exz + ezx) +
                               imu_yz * btyz * (ezy + eyz);
-            const int64_t c = x + SZ * z + SY * j;
-            I.g_lam[c] = R.cell(j, 13)[cidx] + glam;
-            I.g_mu[c] = R.cell(j, 14)[cidx] + gmu;
-            I.g_rho[c] = R.cell(j, 15)[cidx] + grho;
+            const int64_t c = SY * j + cxz;
+            g_lam[c] = R.cell(j, 13)[cidx] + glam;
+            g_mu[c] = R.cell(j, 14)[cidx] + gmu;
+            g_rho[c] = R.cell(j, 15)[cidx] + grho;
         }
         ok = __syncthreads_and(mine) != 0;  // frees halo plane j-2 and cell plane j
         if (!ok) break;

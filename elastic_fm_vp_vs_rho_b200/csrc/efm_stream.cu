@@ -440,6 +440,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     const int iss = stream_issuer(T, nx, W);
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const bool has_src = s_src != 0;
+    unsigned int *const err = I.err;  // read once: the waits' clobbers would reload it
     const Hot H = make_hot(I, 0);
     Row rw[ROWS];
     make_rows<PASS, ROWS>(H, T, x, lx, lr, true, rw);
@@ -459,8 +460,8 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     int issued_hi = min(last, R.p0 + SR - 1);
     bool ok;
     {
-        const bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), I.err) &&
-                          efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), I.err);
+        const bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), err) &&
+                          efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), err);
         ok = __syncthreads_and(mine) != 0;
     }
     for (int j = T.ys; j < T.ye && ok; ++j) {
@@ -489,7 +490,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
                         if (rw[h].in) prefetch_psi(H, Pn, rw[h]);
                 }
             }
-            const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+            const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err);
             if (mine && plane_in) {
                 const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
@@ -540,6 +541,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     const int iss = stream_issuer(T, nx, W);
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const unsigned long long recbits = s_rec;
+    unsigned int *const err = I.err;  // read once: the waits' clobbers would reload it
     const Hot H = make_hot(I, 1);
     float *const border = I.border;
     float *const illum = ILLUM ? I.illum : nullptr;
@@ -567,8 +569,8 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     int issued_hi = min(last, R.p0 + SR - 1);
     bool ok;
     {
-        bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), I.err) &&
-                    efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), I.err);
+        bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), err) &&
+                    efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), err);
         ok = __syncthreads_and(mine) != 0;
     }
     for (int j = T.ys; j < T.ye && ok; ++j) {
@@ -616,7 +618,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     asm volatile("prefetch.global.L1 [%0];" ::"l"(sv + 2 * strip_n + sn));
                 }
             }
-            mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+            mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err);
             if (mine) {
                 const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
 #pragma unroll
@@ -679,7 +681,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                             if (rw[h].in) prefetch_psi(H, Pn, rw[h]);
                     }
                 }
-                const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), I.err);
+                const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err);
                 if (!mine) return false;
                 const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll

@@ -399,3 +399,26 @@ def test_forward_illumination_matches_oracle(golden_c1scale, cuda, stream):
                        float(d["dt"]), float(d["dx"]), tuple(d["src"][0]), d["mt_obs"],
                        (rec[:, 0], rec[:, 1], rec[:, 2]), illumination=True)
     assert rel_err(one, ref) < 1e-4
+
+
+def test_illumination_of_a_heterogeneous_batch_equals_separate_runs(golden_refscale,
+                                                                     golden_c1scale, cuda):
+    """Each instance's illumination volume sits at its own offset of the batch buffer and
+    equals (bit for bit) the volume of a run of that instance alone."""
+    import torch
+
+    from elastic_fm_vp_vs_rho_b200 import ShotBatch
+    a, c = golden_refscale, golden_c1scale
+    both = ShotBatch()
+    _add(both, a, a["lam0"], a["mu0"], a["rho0"], a["mt_obs"], nt=120)
+    _add(both, c, c["lam0"], c["mu0"], c["rho0"], c["mt_obs"])
+    ill = torch.zeros(both.illum_size, dtype=torch.float32, device="cuda")
+    both.forward(illum=ill)
+    both.status()
+    for i, (d, nt) in enumerate(((a, 120), (c, int(c["nt"])))):
+        one = _batch(d, d["lam0"], d["mu0"], d["rho0"], d["mt_obs"], nt=nt)
+        ill1 = torch.zeros(one.illum_size, dtype=torch.float32, device="cuda")
+        one.forward(illum=ill1)
+        one.status()
+        assert float(ill1.abs().max()) > 0
+        assert torch.equal(one.illum_view(ill1, 0), both.illum_view(ill, i))

@@ -431,8 +431,15 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     efm_pdl_trigger();
     const EfmInst &I = insts[efm_find_inst(insts, ninst, block)];
     if (it >= I.nsteps) return;
-    const Tile T = stream_tile<ROWS>(I, block);
+    Tile T = stream_tile<ROWS>(I, block);
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+    if (PASS == EFM_REV) {
+        // the rebuild updates only the box x in [W, nx-W), y in [W, ny-W), z < nz-W and leaves
+        // every other stress as it is: march only over the box planes, skip tiles outside it
+        T.ys = max(T.ys, W);
+        T.ye = min(T.ye, ny - W);
+        if (T.ys >= T.ye || T.z0 >= nz - W || T.x0 >= nx - W || T.x0 + EFM_STX <= W) return;
+    }
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;

@@ -92,8 +92,9 @@ def algorithmic_bytes(w):
     stress:   V(3) + tau(6) + lambda, mu read, tau(6) written = 68 B/cell, plus 24 B per
               cell and active CPML direction (3 memory variables read + written);
     velocity: tau(6) + V(3) + rho read, V(3) written = 52 B/cell + 24 B per CPML direction;
-    reverse velocity: tau(6), V_old(3), 1/rho read, V_new(3) written = 52 B/cell (the
-              one-thread-per-cell kernel also images: 120 B/cell, see imaging);
+    reverse velocity: tau(6), V_old(3), 1/rho read, V_new(3) written = 52 B per cell of
+              the non-CPML box (outside it both ping-pong buffers hold zeros from the
+              first two steps on; the one-thread-per-cell kernel also images);
     imaging: fV_present(3), fV(3), adjoint V(3) and tau(6), lambda, 1/mu, 3 gradients read,
               3 gradients written = 92 B/cell;
     reverse stress: 68 B per cell of the non-CPML box;
@@ -108,7 +109,7 @@ def algorithmic_bytes(w):
         "fwd_velocity": 52 * n + 24 * pml_dirs,
         "adj_stress": 68 * n + 24 * pml_dirs,
         "adj_velocity": 52 * n + 24 * pml_dirs,
-        "rev_velocity": 52 * n,
+        "rev_velocity": 52 * box,
         "imaging": 92 * n,
         "rev_stress": 68 * box,
         "residual_misfit": 12 * ntr,

@@ -539,8 +539,16 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     efm_pdl_trigger();
     const EfmInst &I = insts[efm_find_inst(insts, ninst, block)];
     if (it >= I.nsteps) return;
-    const Tile T = stream_tile<ROWS>(I, block);
+    Tile T = stream_tile<ROWS>(I, block);
     const int nx = I.nx, ny = I.ny, nz = I.nz, W = I.W;
+    if (PASS == EFM_REV && it >= 2) {
+        // the rebuild writes zeros outside the box x in [W, nx-W), y in [W, ny-W), z < nz-W;
+        // from the third step on both ping-pong buffers already hold them there (steps 0 and
+        // 1 wrote them), so only the box planes and the tiles reaching into the box are swept
+        T.ys = max(T.ys, W);
+        T.ye = min(T.ye, ny - W);
+        if (T.ys >= T.ye || T.z0 >= nz - W || T.x0 >= nx - W || T.x0 + EFM_STX <= W) return;
+    }
     const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;

@@ -1,17 +1,20 @@
 #!/usr/bin/env python
 """Benchmark of the hot path: one single-shot FWI gradient evaluation per step.
 
-Workload (the single-shot gradient configuration): 128 x 128 x 96 grid, dx = 10 m,
-seeded layered Vp 2000-5000 m/s + 3 Gaussian anomalies, smoothed initial model, one
-moment-tensor source at 10 Hz, 16 x 16 surface receivers, 1500 time steps, CPML width 10.
-One step = forward modelling with boundary-strip saving + residual/misfit + the adjoint
-pass (reverse-time rebuild, lambda/mu/rho imaging, MT strain) + chain rule to Vp/Vs/rho.
+Default workload (one shot of the learned-preconditioned inversion, the largest
+single-GPU configuration): 256 x 256 x 128 grid, dx = 10 m, seeded layered Vp
+2000-5000 m/s + 3 Gaussian anomalies, smoothed initial model, one moment-tensor source
+at 8 Hz, 48 x 48 surface receivers, 2000 time steps, CPML width 10.  ``--workload
+single-shot`` selects the 128 x 128 x 96, 1500-step, 10 Hz, 16 x 16-receiver gradient
+workload.  One step = forward modelling with boundary-strip saving + residual/misfit +
+the adjoint pass (reverse-time rebuild, lambda/mu/rho imaging, MT strain) + chain rule to
+Vp/Vs/rho.
 
 Metric: Gcell-updates/s, one cell-update = one grid point advanced one time step
 (stress + velocity half-steps).  A step counts ncell * (nt + 2 (nt - 1)) updates: nt
 forward steps, nt-1 adjoint steps and nt-1 reverse rebuild steps.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--nt NT]
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload W]
 
 With N > 1 (torchrun, one rank per GPU) every rank runs its own shot (weak scaling) and
 the gradients and misfits are summed with one NCCL all-reduce per step -- the exchange
@@ -43,8 +46,11 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--nt", type=int, default=1500)
-    p.add_argument("--grid", default="128,128,96", help="nx,ny,nz")
+    p.add_argument("--workload", default="learned-shot", choices=["learned-shot", "single-shot"])
+    p.add_argument("--nt", type=int, default=None, help="record length (workload default)")
+    p.add_argument("--grid", default=None, help="nx,ny,nz (workload default)")
+    p.add_argument("--kernel-reps", type=int, default=100,
+                   help="back-to-back launches per kernel kind for the per-kernel times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-graph", action="store_true",
@@ -58,15 +64,20 @@ def parse():
 # ----------------------------------------------------------------------------- workload
 def workload(args, rank=0):
     from elastic_fm_vp_vs_rho_b200 import configs
-    nx, ny, nz = (int(v) for v in args.grid.split(","))
-    w = configs.single_shot_gradient(seed=2, nx=nx, ny=ny, nz=nz, nt=args.nt)
-    if rank:
-        # weak scaling: every rank its own earthquake position
-        rng = np.random.default_rng(100 + rank)
-        s = w.shots[0]
-        s.sx = int(rng.integers(w.lenpml + 4, nx - w.lenpml - 4))
-        s.sy = int(rng.integers(w.lenpml + 4, ny - w.lenpml - 4))
-    return w
+    if args.workload == "single-shot":
+        nx, ny, nz = (int(v) for v in (args.grid or "128,128,96").split(","))
+        w = configs.single_shot_gradient(seed=2, nx=nx, ny=ny, nz=nz, nt=args.nt or 1500)
+        if rank:
+            # weak scaling: every rank its own earthquake position
+            rng = np.random.default_rng(100 + rank)
+            s = w.shots[0]
+            s.sx = int(rng.integers(w.lenpml + 4, nx - w.lenpml - 4))
+            s.sy = int(rng.integers(w.lenpml + 4, ny - w.lenpml - 4))
+        return w
+    nx, ny, nz = (int(v) for v in (args.grid or "256,256,128").split(","))
+    # weak scaling: rank r takes shot 27 + r of the 8 x 8 source grid
+    return configs.learned_fwi_shot(seed=5, nx=nx, ny=ny, nz=nz, nt=args.nt or 2000,
+                                    shot=(27 + rank) % 64)
 
 
 def cpml_of(w):
@@ -76,14 +87,32 @@ def cpml_of(w):
 
 
 def config_dict(w, args, n):
+    state_mb = 21 * w.ncells * 4 / 1e6
     return {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "nt": w.nt, "dx_m": w.dx,
-            "cpml_width": w.lenpml, "receivers": int(len(w.shots[0].rec_x)), "shots_per_gpu": 1,
+            "fq_hz": w.fq, "cpml_width": w.lenpml, "receivers": int(len(w.shots[0].rec_x)),
+            "shots_per_gpu": 1,
             "step": "forward+misfit+adjoint(rebuild+imaging+MT)+chain rule",
-            "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"shots x{n}"}
+            "l2": f"flushed between timed steps (256 MiB write); the 21 wavefield volumes "
+                  f"({state_mb:.0f} MB) {'exceed' if state_mb > 126 else 'fit in'} the 126 MB L2",
+            "parallelism": f"shots x{n}"}
 
 
 def cell_updates(w):
     return w.ncells * (w.nt + 2 * (w.nt - 1))
+
+
+def minimum_step_bytes(w):
+    """DRAM bytes one step must move at the least, per cell-update: a forward update reads
+    and writes the 9 fields once and reads lambda, mu, rho (84 B) plus 48 B per active CPML
+    direction (6 memory variables read + written); an adjoint step with its reverse-time
+    rebuild is two such updates plus the lambda/mu/rho gradient read-modify-write (192 B)
+    plus the adjoint's CPML (the rebuild has none).  Returns (bytes per step, forward
+    bytes per cell-update)."""
+    nx, ny, nz, W = w.nx, w.ny, w.nz, w.lenpml
+    dirs = (ny * nz * 2 * W + 2 * W * nz * nx + ny * W * nx) / w.ncells
+    fwd = 84.0 + 48.0 * dirs
+    adj = 192.0 + 48.0 * dirs
+    return w.ncells * (w.nt * fwd + (w.nt - 1) * adj), fwd
 
 
 def algorithmic_bytes(w):
@@ -180,7 +209,7 @@ def cpu_baseline_port(args):
     """The FP64 NumPy oracle on a bounded sample of the workload (rank 0, N=1)."""
     import efm_oracle as O
     w = workload(args)
-    nt_s = 6
+    nt_s = max(3, int(6 * 1.6e6 / w.ncells))  # about 10-30 s of FP64 NumPy on one core
     wav = O.ricker(w.fq, w.dt, nt_s)
     cp = cpml_of(w)
     s = w.shots[0]
@@ -316,7 +345,7 @@ def main():
             red[:-1].copy_(g)
             red[-1:].copy_(mis.to(torch.float32))
             dist.all_reduce(red)
-        return g, mis
+        return mod, res, mis, g, mtg
 
     for _ in range(args.warmup):
         step()
@@ -324,6 +353,7 @@ def main():
     if world > 1:
         dist.barrier()
     check = lambda rc: _lib.check(rc)  # noqa: E731
+    check(L.efm_kernel_stats(eng._ctx, None, None, 1))  # count the timed steps' launches
     sampler = ClockSampler(local)
     sampler.start()
     times = []
@@ -339,19 +369,9 @@ def main():
     torch.cuda.synchronize()
     clocks = sampler.stop()
     eng.status()
-    # per-kernel device times: the same steps again with an event pair around every launch
-    # (outside the timed region, which runs without them)
-    stat_steps = min(args.steps, 3)
-    check(L.efm_kernel_stats(eng._ctx, None, None, 1))
-    check(L.efm_set_timing(eng._ctx, 1))
-    for _ in range(stat_steps):
-        flush.fill_(1.0)
-        step()
-    torch.cuda.synchronize()
-    check(L.efm_set_timing(eng._ctx, 0))
-    launches = (__import__("ctypes").c_int64 * _lib.EFM_NKERN)()
-    kms = (__import__("ctypes").c_double * _lib.EFM_NKERN)()
-    check(L.efm_kernel_stats(eng._ctx, launches, kms, 1))
+    ct = __import__("ctypes")
+    launches = (ct.c_int64 * _lib.EFM_NKERN)()
+    check(L.efm_kernel_stats(eng._ctx, launches, None, 1))
     total_ms = sum(times)
     if world > 1:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
@@ -360,19 +380,36 @@ def main():
         dist.barrier()
     upd = cell_updates(w)
     value = world * upd * args.steps / (total_ms * 1e-3) / 1e9
-    # launches per step from the statistics pass (the misfit reduction is two kernels per
-    # call; the chain rule one kernel per step), times the timed steps
-    gpu_launches = (int(sum(launches)) + int(launches[6]) + stat_steps) * args.steps // stat_steps
+    # kernels launched inside the timed steps: the context's counters (graph replays count
+    # their captured launches; the misfit reduction is two kernels per call) plus the chain
+    # rule's one kernel per step
+    gpu_launches = int(sum(launches)) + int(launches[_lib.KERNEL_NAMES.index("residual_misfit")]) \
+        + args.steps
+    per_step = {name: launches[k] / args.steps for k, name in enumerate(_lib.KERNEL_NAMES)
+                if launches[k]}
+
+    # per-kernel device time in sequence: after the timed region, each kernel kind of the
+    # step launched back to back (efm_kernel_time: programmatic launches as in the time
+    # loops, one event pair around all of them), so launch overlap and L2 behaviour match
+    # the step's own sequence rather than isolated launches
+    keep = step()  # loads the gradient's tables (untimed); its buffers stay referenced
+    kt = {}
+    ms = ct.c_double()
+    for name in ("adj_stress+rev_velocity", "rev_stress+adj_velocity", "imaging"):
+        check(L.efm_kernel_time(eng._ctx, _lib.KERNEL_NAMES.index(name), args.kernel_reps,
+                                w.nt // 2, ct.byref(ms), _lib.stream_ptr(None)))
+        kt[name] = ms.value
+    keep += (eng.forward(save_borders=True),)  # loads the forward tables
+    for name in ("fwd_stress", "fwd_velocity"):
+        check(L.efm_kernel_time(eng._ctx, _lib.KERNEL_NAMES.index(name), args.kernel_reps,
+                                w.nt // 2, ct.byref(ms), _lib.stream_ptr(None)))
+        kt[name] = ms.value
+    torch.cuda.synchronize()
+    eng.status()
+    del keep
 
     # roofline of the dominant kernel
     alg = algorithmic_bytes(w)
-    per = {}
-    for k, name in enumerate(_lib.KERNEL_NAMES):
-        if launches[k]:
-            per[name] = {"launches": int(launches[k]), "ms": float(kms[k]),
-                         "avg_us": 1e3 * kms[k] / launches[k],
-                         "gbs": alg[name] / (kms[k] / launches[k] * 1e-3) / 1e9}
-    dom = max(per, key=lambda n: per[n]["ms"])
     peaks = {}
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -380,28 +417,56 @@ def main():
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = None
+    step_ms = total_ms / args.steps
+    per = {}
+    for name, t_ms in kt.items():
+        gbs = alg[name] / (t_ms * 1e-3) / 1e9
+        per[name] = {"launches_per_step": per_step.get(name, 0.0), "us_per_launch": 1e3 * t_ms,
+                     "gbs": gbs, "frac": gbs / peak,
+                     "share_of_step": t_ms * per_step.get(name, 0.0) / step_ms}
+    dom = max(per, key=lambda n: per[n]["share_of_step"])
+    in_seq_ms = sum(p["us_per_launch"] * 1e-3 * p["launches_per_step"] for p in per.values())
+    traffic, traffic_note = None, None
     try:
+        from elastic_fm_vp_vs_rho_b200 import ncu_traffic
         with open(args.traffic_file) as f:
             tf = json.load(f)
-        if tf.get("workload") == w.name and dom in tf.get("bytes_per_launch", {}):
+        if tf.get("workload") != w.name:
+            traffic_note = f"no capture of this workload ({tf.get('workload')} only)"
+        elif tf.get("sources_sha256") != ncu_traffic.sources_sha256():
+            traffic_note = "stale: the kernel sources changed since the ncu capture"
+        elif dom in tf.get("bytes_per_launch", {}):
             traffic = tf["bytes_per_launch"][dom]
+            traffic_note = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch " \
+                           "(profiles/ncu_traffic.json, same kernel sources)"
     except (OSError, ValueError):
-        pass
+        traffic_note = "no ncu capture found"
+    s8d_bytes, s8d_fwd = minimum_step_bytes(w)
+    s8d_gbs = s8d_bytes / (step_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": per[dom]["gbs"], "peak": peak,
                 "unit": "GB/s", "frac": per[dom]["gbs"] / peak,
+                "frac_s8d": s8d_gbs / peak,
+                "frac_s8d_basis": "whole step: minimum DRAM bytes per cell-update (forward "
+                                  f"{s8d_fwd:.1f} B = 84 B + 48 B per active CPML direction; "
+                                  "adjoint + rebuild 192 B + the adjoint's CPML) over the "
+                                  "timed step",
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                 else "fallback 6650 GB/s",
+                "timing": f"in sequence: {args.kernel_reps} back-to-back launches per kernel "
+                          "kind, one event pair (efm_kernel_time), after the timed steps",
                 "algorithmic_bytes_per_launch": alg[dom], "traffic": traffic,
-                "per_kernel": per}
-    # the whole step: algorithmic bytes of every launch of one step (launch counts from the
-    # statistics pass) over the timed step's device time, overlap between launches included
-    step_bytes = sum(alg[name] * launches[k] / stat_steps
-                     for k, name in enumerate(_lib.KERNEL_NAMES) if launches[k] and name in alg)
-    step_gbs = step_bytes / (total_ms / args.steps * 1e-3) / 1e9
+                "traffic_note": traffic_note, "per_kernel": per,
+                "in_sequence_sum_ms_per_step": in_seq_ms, "step_ms": step_ms}
+    # the whole step: algorithmic bytes of every launch of one step (the timed steps' launch
+    # counts) over the timed step's device time, overlap between launches included
+    step_bytes = sum(alg[name] * n for name, n in per_step.items() if name in alg)
+    step_gbs = step_bytes / (step_ms * 1e-3) / 1e9
     roofline["whole_step"] = {"algorithmic_bytes_per_step": step_bytes, "achieved": step_gbs,
                               "frac": step_gbs / peak,
-                              "bytes_per_cell_update": step_bytes / upd}
+                              "bytes_per_cell_update": step_bytes / upd,
+                              "minimum_bytes_per_step": s8d_bytes,
+                              "minimum_bytes_per_cell_update": s8d_bytes / upd,
+                              "frac_minimum_bytes": s8d_gbs / peak}
 
     e2e = None
     if not args.no_e2e:

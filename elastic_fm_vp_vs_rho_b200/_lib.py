@@ -33,6 +33,7 @@ EFM_OPT_RING_DEPTH = 5
 EFM_OPT_PAIR_LAUNCH = 6
 EFM_OPT_PDL = 7
 EFM_OPT_GRAPH = 8
+EFM_OPT_WAIT_LIMIT = 9
 EFM_NKERN = 11
 KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity",
                 "rev_stress", "residual_misfit", "model_reciprocals", "imaging",
@@ -98,6 +99,7 @@ SIGNATURES = {
     "efm_status": (_I, [_P, _P]),
     "efm_set_timing": (_I, [_P, _I]),
     "efm_kernel_stats": (_I, [_P, _P, _P, _I]),
+    "efm_kernel_time": (_I, [_P, _I, _I, _I, _P, _P]),
     "efm_dot": (_I, [_P, _P, _L, _P, _P]),
     "efm_lbfgs_history": (_I, [_P, _P, _P, _P, _I, _L, _I, _P]),
     "efm_lbfgs_direction": (_I, [_P, _P, _P, _P, _P, _I, _L, _I, _P]),

@@ -223,6 +223,25 @@ def single_shot_gradient(seed=2, nx=128, ny=128, nz=96, nt=1500):
                     nt, vp, vs, rho, [shot], vp0, vs0, rho0)
 
 
+def learned_fwi_shot(seed=5, nx=256, ny=256, nz=128, nt=2000, shot=27):
+    """One shot of the learned-preconditioned inversion workload: 256x256x128, dx 10 m,
+    seeded layered Vp 2000-5000 m/s + 3 Gaussian anomalies (+/-10%, sigma 80 m), initial
+    model smoothed with sigma 150 m; shot ``shot`` of the 8x8 surface source grid (z = 4)
+    with a seeded normalised MT and an 8 Hz Ricker, 48x48 surface receivers, 2000 steps."""
+    rng = np.random.default_rng(seed)
+    dx = 10.0
+    vp, vs, rho = layered_anomaly_model(ny, nz, nx, dx, seed)
+    vp0, vs0, rho0 = smooth_model(vp, vs, rho, 150.0 / dx)
+    dt = cfl_dt(dx, float(max(vp.max(), vp0.max())))
+    rx, ry, rz = surface_receivers(nx, ny, 10, 48, 48)
+    sxs = np.linspace(20, nx - 21, 8).astype(int)
+    sys_ = np.linspace(20, ny - 21, 8).astype(int)
+    mts = [random_moment_tensor(rng) for _ in range(64)]
+    sh = Shot(int(sxs[shot % 8]), int(sys_[shot // 8]), 4, tuple(mts[shot]), rx, ry, rz, nt)
+    return Workload(f"single_shot_gradient_{nx}x{ny}x{nz}_nt{nt}", nx, ny, nz, dx, 10, 8.0, dt,
+                    nt, vp, vs, rho, [sh], vp0, vs0, rho0)
+
+
 def batched_inversion(seed=3, nx=200, ny=200, nz=100, nshots=32, nt_range=(1200, 2000)):
     """200x200x100, 32 shots on an 8x4 surface grid, seeded record lengths 1200-2000,
     32x32 receivers, layered + 6 anomalies."""

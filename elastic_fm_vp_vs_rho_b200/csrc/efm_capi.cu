@@ -156,6 +156,11 @@ struct efm_ctx {
     int rows = 2;  // cells per thread of the tables last built for the streaming kernels
     int ring = 4;  // ring depth of those tables' kernels
     int opt_ck_every = 50;
+    unsigned int opt_wait = 0;  // polls per tile wait (0: the kernels' default bound)
+    // kernel kinds whose device tables (and tensor maps) are loaded now, for efm_kernel_time,
+    // and the step count of those tables
+    unsigned int timeable = 0;
+    int time_steps = 0;
     EfmExact *d_ex = nullptr;  // exact-adjoint tables, two (memory-variable parities) per instance
     int ex_cap = 0;
     CUtensorMap *d_maps = nullptr;  // EFM_MAPS_PER_INST per instance
@@ -612,6 +617,7 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
         EfmInst d = base_table(I);
         d.nsteps = I.nt;
         d.err = ctx->d_err;
+        d.wait_lim = ctx->opt_wait;
         for (int c = 0; c < 3; ++c) d.f.v[c] = d.f.vo[c] = I.va(c);
         for (int c = 0; c < 6; ++c) d.f.t[c] = I.tt(c);
         d.gather = gathers ? gathers + I.gather_off : nullptr;
@@ -898,6 +904,7 @@ int efm_clear(efm_ctx *ctx) {
     for (Inst &I : ctx->inst) free_inst(I);
     ctx->inst.clear();
     ctx->layout_ready = false;
+    ctx->timeable = 0;
     drop_loops(ctx);
     return EFM_OK;
 }
@@ -1097,6 +1104,7 @@ int efm_forward_illumination(efm_ctx *ctx, float *gathers, int save, float *illu
     if ((rc = ensure_workspace(ctx, strips || ckpts, strips))) return rc;
     if (ckpts && (rc = ensure_exact(ctx))) return rc;
     bool st = false;
+    ctx->timeable = 0;
     if ((rc = prepare_forward(ctx, gathers, strips, true, s, &st, illum))) return rc;
     int maxnt = 0;
     for (Inst &I : ctx->inst) {
@@ -1134,6 +1142,10 @@ int efm_forward_illumination(efm_ctx *ctx, float *gathers, int save, float *illu
         I.fwd_saved = strips;
         I.ck_saved = ckpts;
     }
+    if (st && illum == nullptr) {
+        ctx->timeable = (1u << EFM_K_FWD_STRESS) | (1u << EFM_K_FWD_VELOCITY);
+        ctx->time_steps = maxnt;
+    }
     return EFM_OK;
 }
 
@@ -1143,6 +1155,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     if (rc) return rc;
     const bool model = (flags & EFM_GRAD_MODEL) != 0, mt = (flags & EFM_GRAD_MT) != 0;
     if (!model && !mt) return fail(EFM_ERR_ARG, "flags select no gradient");
+    ctx->timeable = 0;  // the tables are rebuilt below
     if (flags & EFM_GRAD_EXACT) {
         if (res == nullptr || grad == nullptr || (mt && mtg == nullptr))
             return fail(EFM_ERR_ARG, "null buffer");
@@ -1186,6 +1199,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
         EfmInst a = base_table(I);
         a.nsteps = steps;
         a.err = ctx->d_err;
+        a.wait_lim = ctx->opt_wait;
         for (int c = 0; c < 3; ++c) a.f.v[c] = a.f.vo[c] = I.bv(c);
         for (int c = 0; c < 6; ++c) a.f.t[c] = I.bt(c);
         a.res = res + I.gather_off;
@@ -1219,6 +1233,7 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
             EfmInst r = base_table(I);
             r.nsteps = I.nt - 1;
             r.err = ctx->d_err;
+            r.wait_lim = ctx->opt_wait;
             r.k = -r.k;
             for (int c = 0; c < 3; ++c) {
                 r.f.v[c] = p == 0 ? I.va(c) : I.vb(c);
@@ -1305,6 +1320,67 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
     if (rc) return rc;
     if (model)
         for (Inst &I : ctx->inst) I.fwd_saved = false;  // the rebuild consumed the forward state
+    if (st && model && ctx->opt_pair) {
+        ctx->timeable = (1u << EFM_K_PAIR_ADJS_REVV) | (1u << EFM_K_PAIR_REVS_ADJV) |
+                        (1u << EFM_K_IMAGING);
+        ctx->time_steps = maxsteps;
+    }
+    return EFM_OK;
+}
+
+int efm_kernel_time(efm_ctx *ctx, int kind, int reps, int it, double *ms_per_launch,
+                    void *stream) {
+    if (ctx == nullptr || ms_per_launch == nullptr) return fail(EFM_ERR_ARG, "null argument");
+    if (reps < 1 || reps > 100000) return fail(EFM_ERR_ARG, "reps must be in 1..100000");
+    if (kind < 0 || kind >= EFM_NKERN || !((ctx->timeable >> kind) & 1u))
+        return fail(EFM_ERR_STATE, "the tables of this kernel kind are not loaded (time the "
+                                   "forward kinds after efm_forward, the paired gradient kinds "
+                                   "and the imaging after efm_gradient, streaming kernels only)");
+    if (it < 0 || it + 1 >= ctx->time_steps)
+        return fail(EFM_ERR_ARG, "step index must satisfy 0 <= it and it + 1 < the tables' steps");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = (int)ctx->inst.size();
+    auto dtab = [&](int k) { return (const EfmInst *)(ctx->d_tab + (size_t)k * n); };
+    efm_stream_set_pdl(ctx->opt_pdl);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    EFM_CK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(EFM_ERR_CUDA, "cudaEventCreate failed");
+    }
+    cudaError_t e = cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        const int i = it + (r & 1);  // alternate two steps, as the ping-pong tables do
+        const int kv = (i & 1) ? T_REV_V1 : T_REV_V0, ks = (i & 1) ? T_REV_S1 : T_REV_S0;
+        const int ki = (i & 1) ? T_IMG1 : T_IMG0;
+        switch (kind) {
+            case EFM_K_FWD_STRESS:
+                e = efm_launch_stream(EFM_FWD, 0, ctx->rows, ctx->ring, dtab(T_FWD_S), n,
+                                      ctx->tiles[T_FWD_S], i, s);
+                break;
+            case EFM_K_FWD_VELOCITY:
+                e = efm_launch_stream(EFM_FWD, 1, ctx->rows, ctx->ring, dtab(T_FWD_V), n,
+                                      ctx->tiles[T_FWD_V], i, s);
+                break;
+            case EFM_K_PAIR_ADJS_REVV:
+                e = efm_launch_pair(0, ctx->rows, ctx->ring, dtab(T_ADJ_S), ctx->tiles[T_ADJ_S],
+                                    dtab(kv), ctx->tiles[kv], n, i, s);
+                break;
+            case EFM_K_PAIR_REVS_ADJV:
+                e = efm_launch_pair(1, ctx->rows, ctx->ring, dtab(ks), ctx->tiles[ks],
+                                    dtab(T_ADJ_V), ctx->tiles[T_ADJ_V], n, i, s);
+                break;
+            default: e = efm_launch_image(dtab(ki), n, ctx->tiles[ki], i, s); break;
+        }
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail(EFM_ERR_CUDA, std::string("efm_kernel_time: ") + cudaGetErrorString(e));
+    *ms_per_launch = (double)ms / reps;
     return EFM_OK;
 }
 
@@ -1331,6 +1407,10 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
         case EFM_OPT_RING_DEPTH:
             if (value != 0 && value != 4 && value != 6) return fail(EFM_ERR_ARG, "ring depth must be 0, 4 or 6");
             ctx->opt_ring = value;
+            break;
+        case EFM_OPT_WAIT_LIMIT:
+            if (value < 0) return fail(EFM_ERR_ARG, "wait limit must be >= 0 (0 = default)");
+            ctx->opt_wait = (unsigned int)value;
             break;
         default: return fail(EFM_ERR_ARG, "unknown option");
     }

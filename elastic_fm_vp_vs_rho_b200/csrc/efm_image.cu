@@ -128,16 +128,22 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
     float *const g_lam = I.g_lam, *const g_mu = I.g_mu, *const g_rho = I.g_rho;
     const int cxz = x + nx * z;
     const float idt = I.inv_dt, idx = I.inv_dx;
+    unsigned int *const err = I.err;
+    const uint32_t wl = I.wait_lim;
+    // oldest halo / cell plane no block-wide wait has confirmed yet (the drain after a wait
+    // that gave up starts there: older stages may be two phases further)
+    int hpend = R.p0, cpend = R.c0;
     bool ok;
     {
         bool mine = true;
-        for (int p = R.p0; p < ys; ++p) mine = mine && efm_mbar_wait(&hbar[R.hs(p)], R.hpar(p), I.err);
-        mine = mine && efm_mbar_wait(&hbar[R.hs(ys)], R.hpar(ys), I.err);
+        for (int p = R.p0; p < ys; ++p) mine = mine && efm_mbar_wait(&hbar[R.hs(p)], R.hpar(p), err, wl);
+        mine = mine && efm_mbar_wait(&hbar[R.hs(ys)], R.hpar(ys), err, wl);
         ok = __syncthreads_and(mine) != 0;
+        if (ok) hpend = ys + 1;
     }
     for (int j = ys; j < ye && ok; ++j) {
-        const bool mine = efm_mbar_wait(&hbar[R.hs(j + 1)], R.hpar(j + 1), I.err) &&
-                          efm_mbar_wait(&cbar[R.cs(j)], R.cpar(j), I.err);
+        const bool mine = efm_mbar_wait(&hbar[R.hs(j + 1)], R.hpar(j + 1), err, wl) &&
+                          efm_mbar_wait(&cbar[R.cs(j)], R.cpar(j), err, wl);
         if (mine && colin && j >= EFM_HS && j < ny - EFM_HS) {
             const float *px = R.halo(j, 0), *py = R.halo(j, 1), *pz = R.halo(j, 2), *rm = R.halo(j, 3);
             const float pxc = px[hidx], pyc = py[hidx], pzc = pz[hidx];
@@ -181,6 +187,8 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         }
         ok = __syncthreads_and(mine) != 0;  // frees halo plane j-2 and cell plane j
         if (!ok) break;
+        hpend = j + 2;
+        cpend = j + 1;
         if (threadIdx.x == 0) {
             if (j - 2 + IMG_RH <= hlast) issue_halo(R, tm, x0, z0, j - 2 + IMG_RH);
         } else if (threadIdx.x == 32) {
@@ -190,8 +198,8 @@ efm_image_stream(const EfmInst *__restrict__ insts, int ninst, int it) {
         if (j + IMG_RC <= clast) c_hi = j + IMG_RC;
     }
     if (!ok) {
-        for (int p = R.p0; p <= h_hi; ++p) efm_mbar_wait(&hbar[R.hs(p)], R.hpar(p), nullptr);
-        for (int p = R.c0; p <= c_hi; ++p) efm_mbar_wait(&cbar[R.cs(p)], R.cpar(p), nullptr);
+        for (int p = hpend; p <= h_hi; ++p) efm_mbar_wait(&hbar[R.hs(p)], R.hpar(p), nullptr);
+        for (int p = cpend; p <= c_hi; ++p) efm_mbar_wait(&cbar[R.cs(p)], R.cpar(p), nullptr);
     }
 }
 

@@ -78,7 +78,8 @@ k_noalloc_finish(const double *__restrict__ partials, int nblk, double *__restri
 
 // Device address of g_noalloc_partials, looked up once per device.  In host code the
 // array's name only stands for the symbol; the kernels need the address the runtime
-// reports for the current device.
+// reports for the current device.  The cache is never refreshed: a cudaDeviceReset of a
+// device (which ends its context and frees the module's array) leaves that entry stale.
 std::mutex g_noalloc_mu;
 double *g_noalloc_addr[64] = {};
 

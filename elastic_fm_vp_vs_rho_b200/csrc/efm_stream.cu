@@ -116,6 +116,11 @@ __device__ __forceinline__ Tile stream_tile(const EfmInst &I, int block) {
     return t;
 }
 
+// After a wait gave up: wait (with the default bound) for the loads still in flight, planes
+// first..last, so that no TMA write into this block's shared memory outlives the block.
+// `first` is the oldest plane no block-wide wait has confirmed; planes in flight occupy
+// distinct stages whose current phase is theirs, so each wait is well defined (an older
+// plane's stage may already be two phases further, where its parity would be ambiguous).
 template <int ROWS, int SR>
 __device__ void drain(const Ring<ROWS, SR> &R, int first, int last) {
     for (int p = first; p <= last; ++p) efm_mbar_wait(&R.bar[R.stage(p)], R.parity(p), nullptr);
@@ -448,6 +453,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const bool has_src = s_src != 0;
     unsigned int *const err = I.err;  // read once: the waits' clobbers would reload it
+    const uint32_t wl = I.wait_lim;
     const Hot H = make_hot(I, 0);
     Row rw[ROWS];
     make_rows<PASS, ROWS>(H, T, x, lx, lr, true, rw);
@@ -465,11 +471,13 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
     }
     const int last = T.ye;
     int issued_hi = min(last, R.p0 + SR - 1);
+    int pend = R.p0;  // oldest plane no block-wide wait has confirmed yet
     bool ok;
     {
-        const bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), err) &&
-                          efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), err);
+        const bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), err, wl) &&
+                          efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), err, wl);
         ok = __syncthreads_and(mine) != 0;
+        if (ok) pend = T.ys + 1;
     }
     for (int j = T.ys; j < T.ye && ok; ++j) {
         const bool plane_in = j >= EFM_HS && j < ny - EFM_HS && !(PASS == EFM_REV && (j < W || j >= ny - W));
@@ -497,7 +505,7 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
                         if (rw[h].in) prefetch_psi(H, Pn, rw[h]);
                 }
             }
-            const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err);
+            const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err, wl);
             if (mine && plane_in) {
                 const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
@@ -518,12 +526,13 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
         const bool mine = wpml ? plane(Tag<true>{}) : plane(Tag<false>{});
         ok = __syncthreads_and(mine) != 0;  // frees plane j-1's stage; uniform timeout exit
         if (!ok) break;
+        pend = j + 2;
         if ((int)threadIdx.x == iss)
             advance<ROWS, SR, NH, NC>(R, tm, tm + NH + 1, 1, 6, plane_in, T.x0, T.z0, j, last);
         if (j - 1 + SR <= last) issued_hi = j - 1 + SR;
     }
     if ((int)threadIdx.x == iss) efm_bulk_wait_all();
-    if (!ok) drain(R, R.p0, issued_hi);  // no load may still target this block's smem
+    if (!ok) drain(R, pend, issued_hi);  // no load may still target this block's smem
 }
 
 // halo fields: txx tzz txy txz tyz 1/rho ; center fields: tyy vx vy vz   (forward / adjoint);
@@ -557,6 +566,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const unsigned long long recbits = s_rec;
     unsigned int *const err = I.err;  // read once: the waits' clobbers would reload it
+    const uint32_t wl = I.wait_lim;
     const Hot H = make_hot(I, 1);
     float *const border = I.border;
     float *const illum = ILLUM ? I.illum : nullptr;
@@ -582,11 +592,13 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
     const CUtensorMap *stm = PASS == EFM_REV ? tm + NH + NC : tm + NH + 1;
     const int last = T.ye;
     int issued_hi = min(last, R.p0 + SR - 1);
+    int pend = R.p0;  // oldest plane no block-wide wait has confirmed yet
     bool ok;
     {
-        bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), err) &&
-                    efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), err);
+        bool mine = efm_mbar_wait(&bars[R.stage(R.p0)], R.parity(R.p0), err, wl) &&
+                    efm_mbar_wait(&bars[R.stage(T.ys)], R.parity(T.ys), err, wl);
         ok = __syncthreads_and(mine) != 0;
+        if (ok) pend = T.ys + 1;
     }
     for (int j = T.ys; j < T.ye && ok; ++j) {
         const int y = j;
@@ -633,7 +645,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                     asm volatile("prefetch.global.L1 [%0];" ::"l"(sv + 2 * strip_n + sn));
                 }
             }
-            mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err);
+            mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err, wl);
             if (mine) {
                 const int s0 = R.stage(j), sp = R.stage(j + 1), sm = R.stage(j - 1);
 #pragma unroll
@@ -696,7 +708,7 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
                             if (rw[h].in) prefetch_psi(H, Pn, rw[h]);
                     }
                 }
-                const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err);
+                const bool mine = efm_mbar_wait(&bars[R.stage(j + 1)], R.parity(j + 1), err, wl);
                 if (!mine) return false;
                 const int sm = R.stage(j - 1), s0 = R.stage(j), sp = R.stage(j + 1);
 #pragma unroll
@@ -818,12 +830,13 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
         }
         ok = __syncthreads_and(mine) != 0;
         if (!ok) break;
+        pend = j + 2;
         if ((int)threadIdx.x == iss)
             advance<ROWS, SR, NH, NC>(R, tm, stm, 1, 3, store, T.x0, T.z0, j, last);
         if (j - 1 + SR <= last) issued_hi = j - 1 + SR;
     }
     if ((int)threadIdx.x == iss) efm_bulk_wait_all();
-    if (!ok) drain(R, R.p0, issued_hi);
+    if (!ok) drain(R, pend, issued_hi);
 }
 
 template <int PASS, int ROWS, int SR>

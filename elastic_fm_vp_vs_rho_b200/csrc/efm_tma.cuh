@@ -1,15 +1,16 @@
 // Thin inline-PTX layer for the plane-streaming kernels: mbarriers, TMA tile loads and stores.
 //
 // Only plain (non-multicast) cp.async.bulk.tensor loads and stores on this GPU's own memory
-// are issued.  Every mbarrier wait is bounded: after EFM_WAIT_LIMIT polls it gives up, sets the
-// context's error word and lets the caller drain and return, so a lost transfer reports an
-// error instead of hanging the GPU.
+// are issued.  Every mbarrier wait is bounded: after EFM_WAIT_LIMIT polls (or the context's
+// shorter limit, EFM_OPT_WAIT_LIMIT) it gives up, sets the context's error word and lets the
+// caller drain and return, so a lost transfer reports an error instead of hanging the GPU.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #define EFM_WAIT_LIMIT (1u << 22)
+#define EFM_WAIT_HINT_NS 32u  // suspend-time hint of one poll under a context wait limit
 #define EFM_ERR_FLAG_TIMEOUT 1u
 
 __device__ __forceinline__ uint32_t efm_smem_addr(const void *p) {
@@ -43,11 +44,32 @@ __device__ __forceinline__ bool efm_mbar_try_wait(uint64_t *bar, uint32_t parity
     return ok != 0;
 }
 
-// Wait for phase `parity` of `bar`; false after EFM_WAIT_LIMIT polls (error flag set).
+// One poll that suspends the thread for at most about `ns` nanoseconds.
+__device__ __forceinline__ bool efm_mbar_try_wait_ns(uint64_t *bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(efm_smem_addr(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of `bar`.  lim == 0: up to EFM_WAIT_LIMIT polls (the default);
+// lim > 0: up to lim polls of about EFM_WAIT_HINT_NS each -- a limit a failure-detection test
+// sets so short that a tile still in flight makes the wait give up.  False when it gave up
+// (error flag set).
 __device__ __forceinline__ bool efm_mbar_wait(uint64_t *bar, uint32_t parity,
-                                              unsigned int *err_flag) {
-    for (uint32_t i = 0; i < EFM_WAIT_LIMIT; ++i)
-        if (efm_mbar_try_wait(bar, parity)) return true;
+                                              unsigned int *err_flag, uint32_t lim = 0) {
+    if (lim == 0) {
+        for (uint32_t i = 0; i < EFM_WAIT_LIMIT; ++i)
+            if (efm_mbar_try_wait(bar, parity)) return true;
+    } else {
+        for (uint32_t i = 0; i < lim; ++i)
+            if (efm_mbar_try_wait_ns(bar, parity, EFM_WAIT_HINT_NS)) return true;
+    }
     if (err_flag) atomicOr(err_flag, EFM_ERR_FLAG_TIMEOUT);
     return false;
 }

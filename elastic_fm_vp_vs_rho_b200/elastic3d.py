@@ -313,6 +313,28 @@ class Alpha:
 
 
 # ============================================================================ Elastic3D
+def reduce_shard(grads, misfits, shape, want_grad, device):
+    """Sum of this rank's shots, then over all ranks with one collective.
+
+    grads: this rank's per-shot (3, ny, nz, nx) lambda/mu/rho gradients (empty when
+    ``want_grad`` is false or the rank holds no shot); misfits: float64 tensor of its
+    per-shot misfits.  Returns (total misfit over every shot of every rank, summed float32
+    gradient or None).  The reference gathers the per-shot gradients to rank 0 with
+    Send/Recv and reduces the misfit (mainPropElastic3D_MT.py:2425-2475); here every rank
+    gets the sums, so every rank can take the same L-BFGS step.
+    """
+    torch = _torch()
+    tot = misfits.sum().reshape(1).to(torch.float64)
+    if not want_grad:
+        (tot,) = _dist.all_reduce_sum(tot)
+        return float(tot.item()), None
+    acc = torch.zeros((3,) + tuple(shape), dtype=torch.float32, device=device)
+    for g in grads:
+        acc += g
+    acc, tot = _dist.all_reduce_sum(acc, tot)
+    return float(tot.item()), acc
+
+
 class Elastic3D:
     """Forward modelling, misfit, adjoint gradients and the two inversion drivers
     (:1432-2720), on the GPU.
@@ -570,24 +592,14 @@ class Elastic3D:
     def _shots_misfit(self, eng, obs_flat, want_grad):
         """Forward all shots; optionally the summed lambda/mu/rho gradient."""
         torch = _torch()
-        if len(eng) == 0:  # a rank without shots still joins the collectives
-            acc = torch.zeros((3, self.ny, self.nz, self.nx), dtype=torch.float32, device="cuda")
-            tot = torch.zeros(1, dtype=torch.float64, device="cuda")
-        else:
+        grads, mis = [], torch.zeros(0, dtype=torch.float64, device="cuda")
+        if len(eng) > 0:  # a rank without shots still joins the collectives
             mod = eng.forward(save_borders=want_grad)
             res, mis = eng.residual_misfit(mod, obs_flat)
-            tot = mis.sum().reshape(1)
-            acc = torch.zeros((3, self.ny, self.nz, self.nx), dtype=torch.float32, device="cuda")
             if want_grad:
                 g, _ = eng.gradient(res, model=True)
-                for i in range(len(eng)):
-                    acc += eng.grad_view(g, i)
-        # one collective per call: gradients (when wanted) + misfit summed over ranks
-        if want_grad:
-            acc, tot = _dist.all_reduce_sum(acc, tot)
-            return float(tot.item()), acc
-        (tot,) = _dist.all_reduce_sum(tot)
-        return float(tot.item()), None
+                grads = [eng.grad_view(g, i) for i in range(len(eng))]
+        return reduce_shard(grads, mis, (self.ny, self.nz, self.nx), want_grad, "cuda")
 
     def _update_vp_vs_rho(self, cRho_top):
         """compute_Vp_Vs with the current rho, compute_Rho, keep rho's top 10 planes

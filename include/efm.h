@@ -174,16 +174,21 @@ EFM_API int efm_residual_misfit(const efm_ctx *ctx, const float *mod_dev, const 
  * a fixed array compiled into libefm.so (EFM_NOALLOC_MAX_SEGMENTS x 256 float64 partial
  * sums, 128 KiB), which every GPU that loads the library holds until the process exits.
  *
- * seg_host: nseg + 1 non-decreasing float offsets into mod/obs/res (segment i is
+ * seg_host: nseg + 1 non-decreasing int64 element offsets into mod/obs/res (segment i is
  * [seg_host[i], seg_host[i+1]), e.g. the instances of a context: efm_gather_offset);
  * 1 <= nseg <= EFM_NOALLOC_MAX_SEGMENTS, larger nseg is rejected with EFM_ERR_ARG.
  * misfit_dev: [nseg] float64, 0.5 * sum(res^2) per segment.
  *
  * The first call on each device looks up the scratch array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call before any stream
- * capture.  Every call shares the array and it keeps the last call's contents (each call
- * writes all the partials it reads, so nothing needs clearing); calls that overlap on the
- * GPU race on it and must not be issued.
+ * capture.  With lazy module loading (the CUDA default since 12.2) that first call is also
+ * when the driver loads the library's module onto the device and reserves the 128 KiB, so
+ * a caller that reserves all of the GPU's memory for its own pool makes the first call
+ * before reserving it.  The address is cached per device ordinal for the life of the
+ * process: after cudaDeviceReset it is stale, and this entry point must not be called again
+ * on that device.  Every call shares the array and it keeps the last call's contents (each
+ * call writes all the partials it reads, so nothing needs clearing); calls that overlap on
+ * the GPU race on it and must not be issued.
  */
 #define EFM_NOALLOC_MAX_SEGMENTS 64
 EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_dev,
@@ -218,6 +223,13 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
  * the same (kernel counters still count every launch); 0: launched step by step.  Loops
  * run with efm_set_timing(ctx, 1) are always launched step by step. */
 #define EFM_OPT_GRAPH 8
+/* Bound of every tile wait of the plane-streaming kernels: 0 (default) = 2^22 polls; n > 0 =
+ * n polls of about 32 ns each.  A wait that runs out sets the context's error word
+ * (efm_status -> EFM_ERR_TIMEOUT), waits for its block's own loads still in flight and
+ * returns; the call completes with invalid outputs, and the next call with the default
+ * limit is unaffected.  Small values exist for failure-detection tests (no reference
+ * counterpart; the reference's kernels have no waits). */
+#define EFM_OPT_WAIT_LIMIT 9
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*
@@ -253,10 +265,28 @@ EFM_API int efm_set_timing(efm_ctx *ctx, int enable);
  * kernel kind since the last reset; arrays of EFM_NKERN.  Synchronizes the recorded events.
  */
 EFM_API int efm_kernel_stats(efm_ctx *ctx, int64_t *launches, double *ms, int reset);
+/*
+ * In-sequence device time of one kernel kind: `reps` launches of it back to back on
+ * `stream` (programmatic launches as in the time loops, steps it and it+1 alternating),
+ * one event pair around all of them; *ms_per_launch = their time / reps.  Kinds: the
+ * forward stress / velocity after efm_forward, the two paired gradient launches and the
+ * imaging after efm_gradient (plane-streaming kernels, paired launches); others give
+ * EFM_ERR_STATE.  The launches overwrite the context's wavefields and add into the last
+ * gradient buffer: run efm_forward again before the next efm_gradient.  No reference
+ * counterpart (measurement only).
+ */
+EFM_API int efm_kernel_time(efm_ctx *ctx, int kind, int reps, int it, double *ms_per_launch,
+                            void *stream);
 
 /* ---------------------------------------------------------------- volume utilities */
 
-/* out[0] = sum(a*b) in float64 (the dot products of L_BFGS, lbfgs.py:39-65). */
+/*
+ * out[0] = sum(a*b) in float64 (the dot products of L_BFGS, lbfgs.py:39-65).
+ * efm_dot and efm_lbfgs_direction share one scratch area per device (block partial sums and
+ * the segment bounds, allocated on first use): calls of either that may overlap on the GPU
+ * (issued on different streams without an ordering between them) race on it; issue them on
+ * one stream or order the streams.
+ */
 EFM_API int efm_dot(const float *a_dev, const float *b_dev, int64_t n, double *out_dev, void *stream);
 
 /*

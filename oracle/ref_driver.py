@@ -9,7 +9,15 @@ of ``Elastic3D`` that drive them, launch for launch:
 
 * ``forward``   = Elastic3D.forwardFields('mod', mode 1)  (mainPropElastic3D_MT.py:1812-1847)
 * ``gradient``  = Elastic3D.backwardFields_FowardFieldsRemake  (:1929-2054)
+* ``mt_gradient`` = Elastic3D.backwardFields in mode 0 (:2056-2082) with
+  computeGradients_Mij (:1902-1920)
 * residual / misfit = computeResidual + computeCostFunction  (:2128-2142)
+
+An instance may hold several sources (the uneven-batch workload places one to four
+moment tensors in one model).  The reference drives one earthquake per Elastic3D; here
+each step injects every source with addSource's arithmetic (:1728-1734), one source after
+the other in list order, and the MT gradient runs kernel_Gradients_Mij once per source
+on the shared adjoint field.  With one source this is the reference's sequence exactly.
 
 including the reference's full-volume CPML memory variables, border buffers, the three
 DTD copies, nine CPML zeroings per reverse step and the host accumulation of the three
@@ -37,8 +45,12 @@ class RefCPUSolver:
         self.w = f(np.asarray(wavelet).reshape(-1))
         self.nt = len(self.w)
         self.dt, self.dx = np.float32(dt), np.float32(dx)
-        self.src = [int(v) for v in src]
-        self.mt = [float(v) for v in mt]
+        src = np.asarray(src, np.int64)
+        mt = np.asarray(mt, np.float64)
+        self.srcs = [tuple(int(v) for v in row) for row in src.reshape(-1, 3)]
+        self.mts = [[float(v) for v in row] for row in mt.reshape(-1, 6)]
+        if len(self.srcs) != len(self.mts):
+            raise ValueError("one moment tensor per source")
         self.rx, self.ry, self.rz = (np.ascontiguousarray(a, np.int32) for a in rec)
         self.nsta = len(self.rx)
         self.W = int(lenpml)
@@ -89,11 +101,11 @@ class RefCPUSolver:
                                self.nx, self.ny, self.nz, grid=self.grid3, block=self.block3)
 
     def _source(self, F, it, sign):
-        # addSource (:1728-1734): six scalar adds of float32(sign * M_ij * w[it])
-        sx, sy, sz = self.src
-        for name, m in zip(("Tauxx", "Tauyy", "Tauzz", "Tauxy", "Tauxz", "Tauyz"), self.mt):
-            v = np.float32(np.float32(sign * m) * self.w[it])
-            F[name][sy, sz, sx] = np.float32(F[name][sy, sz, sx] + v)
+        # addSource (:1728-1734): six scalar adds of float32(sign * M_ij * w[it]) per source
+        for (sx, sy, sz), mt in zip(self.srcs, self.mts):
+            for name, m in zip(("Tauxx", "Tauyy", "Tauzz", "Tauxy", "Tauxz", "Tauyz"), mt):
+                v = np.float32(np.float32(sign * m) * self.w[it])
+                F[name][sy, sz, sx] = np.float32(F[name][sy, sz, sx] + v)
 
     def _border(self, fn, F, Bx, it):
         for comp in ("Vx", "Vy", "Vz"):
@@ -164,3 +176,26 @@ class RefCPUSolver:
                                    self.ny, self.nz, grid=self.grid3, block=self.block3)
             gM += dM
         return gL, gM, gR
+
+    def mt_gradient(self, res):
+        """backwardFields in mode 0 (:2056-2082): nt adjoint steps with residual injection,
+        then kernel_Gradients_Mij at every source (:1902-1920); the six float32 products
+        of each step are added into float64 totals as the host does.  Returns (nsrc, 6)."""
+        B = self._fields()
+        res = np.ascontiguousarray(res, np.float32)
+        kk = self.k
+        gg = np.zeros((6, 1), np.float32)
+        tot = np.zeros((len(self.srcs), 6), np.float64)
+        for it in range(self.nt):
+            self._tau(B, +1)
+            self._vel(B, +1)
+            kk.kernel_add_adjoint_source(B["Vx"], res[0], B["Vy"], res[1], B["Vz"], res[2],
+                                         self.rx, self.ry, self.rz, self.nsta, self.nt, it,
+                                         self.nx, self.nz, grid=self.grid_st, block=(TBX, 1, 1))
+            for q, (sx, sy, sz) in enumerate(self.srcs):
+                kk.kernel_Gradients_Mij(B["Tauxx"], B["Tauyy"], B["Tauzz"], B["Tauxy"],
+                                        B["Tauxz"], B["Tauyz"], self.w, self.vp, self.vs,
+                                        self.rho, self.lam, self.mu, gg, sx, sy, sz, self.nt,
+                                        it, self.nx, self.nz, grid=(1, 1, 1), block=(TBX, 1, 1))
+                tot[q] += gg.reshape(-1).astype(np.float64)
+        return tot

@@ -82,7 +82,15 @@ def _case_inputs(name):
 
 
 def run_case(main, name, with_fwi):
-    c = _case_inputs(name)
+    return run_inputs(main, _case_inputs(name), with_fwi)
+
+
+def run_inputs(main, c, with_fwi):
+    """Drive the reference's own classes on one case.  ``c`` holds the grid, the true
+    model, sources, receivers and time axis; optional keys: ``mt_obs`` / ``mt_mod`` (the
+    observed and the starting moment tensor), ``init`` (Vp, Vs, rho of the starting model
+    instead of the true model smoothed with ``sigma`` cells), ``rec`` (receiver x, y, z
+    instead of an nrx x nry surface grid)."""
     nx, ny, nz, dx, lenpml, fq = c["nx"], c["ny"], c["nz"], c["dx"], c["lenpml"], c["fq"]
     srcs = c["srcs"]
     ref_harness.set_globals(main, nx=nx, ny=ny, nz=nz, fq=fq, nSismos=len(srcs))
@@ -103,7 +111,10 @@ def run_case(main, name, with_fwi):
     wavelet.ricker()
     cpml = main.CPML(lenpml, wavelet, m_true)
 
-    rx, ry, rz = configs.surface_receivers(nx, ny, lenpml, c["nrx"], c["nry"])
+    if "rec" in c:
+        rx, ry, rz = (np.asarray(a, np.int32) for a in c["rec"])
+    else:
+        rx, ry, rz = configs.surface_receivers(nx, ny, lenpml, c["nrx"], c["nry"])
     geometry = main.Geometry()
     for (sx, sy, sz) in srcs:
         geometry.addSismo(main.Earthquake(sx, sy, sz))
@@ -111,16 +122,17 @@ def run_case(main, name, with_fwi):
         for i in range(len(rx)):
             geometry.sismos[k].addStation(main.Station(int(rx[i]), int(ry[i]), int(rz[i])))
 
-    m_obs = main.StressTensor(0.8, -0.3, 0.5, 0.4, -0.2, 0.3)
-    m_mod = main.StressTensor(0.5, 0.0, 0.5, 0.0, 0.5, 0.0)
+    mt_obs = [float(v) for v in c.get("mt_obs", (0.8, -0.3, 0.5, 0.4, -0.2, 0.3))]
+    mt_mod = [float(v) for v in c.get("mt_mod", (0.5, 0.0, 0.5, 0.0, 0.5, 0.0))]
+    m_obs = main.StressTensor(*mt_obs)
+    m_mod = main.StressTensor(*mt_mod)
 
     out.update(dict(nx=nx, ny=ny, nz=nz, dx=dx, lenpml=lenpml, fq=fq, dt=wavelet.dt,
                     vmax=np.float64(m_true.VmaxVp),
                     nt=wavelet.nSamples, waveform=wavelet.waveform.ravel().copy(),
                     ax=cpml.ax, bx=cpml.bx, ay=cpml.ay, by=cpml.by, az=cpml.az, bz=cpml.bz,
                     src=np.array(srcs, np.int32), rec_x=rx, rec_y=ry, rec_z=rz,
-                    mt_obs=np.array([0.8, -0.3, 0.5, 0.4, -0.2, 0.3]),
-                    mt_mod=np.array([0.5, 0.0, 0.5, 0.0, 0.5, 0.0]),
+                    mt_obs=np.array(mt_obs), mt_mod=np.array(mt_mod),
                     lam_true=m_true.Lambda, mu_true=m_true.Mu, rho_true=m_true.Rho))
 
     # observed data: true model, true MT, forwardFields('obs') (:1812-1847)
@@ -139,9 +151,12 @@ def run_case(main, name, with_fwi):
     # initial model: smoothed true model
     from scipy.ndimage import gaussian_filter
     cn = main.Model(nz, ny, nx, dx, dx, dx)
-    cn.Vp = gaussian_filter(m_true.Vp, sigma=c["sigma"])
-    cn.Vs = gaussian_filter(m_true.Vs, sigma=c["sigma"])
-    cn.Rho = gaussian_filter(m_true.Rho, sigma=c["sigma"])
+    if "init" in c:
+        cn.Vp, cn.Vs, cn.Rho = (np.array(a, np.float32) for a in c["init"])
+    else:
+        cn.Vp = gaussian_filter(m_true.Vp, sigma=c["sigma"])
+        cn.Vs = gaussian_filter(m_true.Vs, sigma=c["sigma"])
+        cn.Rho = gaussian_filter(m_true.Rho, sigma=c["sigma"])
     cn.compute_Lambda_Mu()
     cn.hostToDevice()
     out.update(lam0=cn.Lambda, mu0=cn.Mu, rho0=cn.Rho)

@@ -59,6 +59,9 @@ def test_argument_errors_return_status():
         # no instances: a forward is a state error, not a crash
         assert L.efm_forward(ctx, None, 0, None) != _lib.EFM_OK
         assert L.efm_num_instances(ctx) == 0
+        assert L.efm_set_option(ctx, _lib.EFM_OPT_WAIT_LIMIT, -1) == _lib.EFM_ERR_ARG
+        assert L.efm_set_option(ctx, _lib.EFM_OPT_WAIT_LIMIT, 4) == _lib.EFM_OK
+        assert L.efm_set_option(ctx, _lib.EFM_OPT_WAIT_LIMIT, 0) == _lib.EFM_OK
         assert L.efm_smooth_mask(None, None, 1, 1, 1, 1.0, 0, 0, None) == _lib.EFM_ERR_ARG
         assert L.efm_lbfgs_history(None, None, None, None, 1, 0, 0, None) == _lib.EFM_ERR_ARG
     finally:

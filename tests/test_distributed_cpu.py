@@ -45,6 +45,19 @@ def _worker(rank, ws, port, mode, q):
             mis += 0.5 * (k + 1) ** 2
         if mode == "fail" and rank == 1:
             raise RuntimeError("simulated lost shot on rank 1")
+        if mode == "driver":
+            # the FWI driver's own reduction (Elastic3D._shots_misfit -> reduce_shard) over
+            # per-shot gradients and misfits of this rank's contiguous shot range
+            from elastic_fm_vp_vs_rho_b200.elastic3d import reduce_shard
+            lo, hi = D.shard(5)  # rank / world size from the process group
+            shape = (4, 3, 5)
+            grads = [(k + 1) * torch.arange(180, dtype=torch.float32).reshape(3, *shape)
+                     for k in range(lo, hi)]
+            mis = torch.tensor([0.5 * (k + 1) ** 2 for k in range(lo, hi)], dtype=torch.float64)
+            tot, acc = reduce_shard(grads, mis, shape, True, "cpu")
+            tot2, none = reduce_shard([], mis, shape, False, "cpu")
+            q.put((rank, "ok", float(acc[2, 3, 2, 4]), tot, tot2, none is None, hi - lo))
+            return
         gs, ms = D.all_reduce_sum(g, mis)
         q.put((rank, "ok", float(gs[0, 0, 0]), float(ms[0])))
     except Exception as e:  # reported to the parent
@@ -89,3 +102,19 @@ def test_lost_rank_surfaces_as_error_not_hang():
     out = _run("fail")
     assert out[1][1] == "error" and "simulated lost shot" in out[1][3]
     assert out[0][1] == "error"  # rank 0's all-reduce ends with an error within the timeout
+
+
+def test_fwi_driver_reduction_world2():
+    """Elastic3D's sharded reduction with two gloo ranks: 5 shots split 3 + 2, per-shot
+    gradients and misfits summed on each rank, then over ranks in one collective."""
+    out = _run("driver")
+    total_scale = sum(k + 1 for k in range(5))
+    total_m = sum(0.5 * (k + 1) ** 2 for k in range(5))
+    for r in (0, 1):
+        assert out[r][1] == "ok", out[r]
+    assert sorted(out[r][6] for r in (0, 1)) == [2, 3]
+    for r in (0, 1):
+        assert out[r][2] == pytest.approx(179 * total_scale)  # last element of the arange
+        assert out[r][3] == pytest.approx(total_m)
+        assert out[r][4] == pytest.approx(total_m)
+        assert out[r][5]

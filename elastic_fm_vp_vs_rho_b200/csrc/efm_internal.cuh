@@ -73,7 +73,7 @@ struct EfmInst {
     // 1/rho, and a byte per (plane, tile) telling whether the tile holds a receiver
     const CUtensorMap *tmap;
     unsigned int *err;
-    unsigned int wait_lim;  // polls per tile wait (0: the default bound; see efm_tma.cuh)
+    unsigned int wait_lim;  // polls per tile wait (0: the default bound; efm_mbar_wait)
     const float *rmu, *buoy;
     const uint8_t *rec_tile;
 };

@@ -10,7 +10,6 @@
 #include <stdint.h>
 
 #define EFM_WAIT_LIMIT (1u << 22)
-#define EFM_WAIT_HINT_NS 32u  // suspend-time hint of one poll under a context wait limit
 #define EFM_ERR_FLAG_TIMEOUT 1u
 
 __device__ __forceinline__ uint32_t efm_smem_addr(const void *p) {
@@ -44,23 +43,23 @@ __device__ __forceinline__ bool efm_mbar_try_wait(uint64_t *bar, uint32_t parity
     return ok != 0;
 }
 
-// One poll that suspends the thread for at most about `ns` nanoseconds.
-__device__ __forceinline__ bool efm_mbar_try_wait_ns(uint64_t *bar, uint32_t parity, uint32_t ns) {
+// One poll that never suspends the thread.
+__device__ __forceinline__ bool efm_mbar_test_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(efm_smem_addr(bar)), "r"(parity), "r"(ns)
+        : "r"(efm_smem_addr(bar)), "r"(parity)
         : "memory");
     return ok != 0;
 }
 
-// Wait for phase `parity` of `bar`.  lim == 0: up to EFM_WAIT_LIMIT polls (the default);
-// lim > 0: up to lim polls of about EFM_WAIT_HINT_NS each -- a limit a failure-detection test
-// sets so short that a tile still in flight makes the wait give up.  False when it gave up
-// (error flag set).
+// Wait for phase `parity` of `bar`.  lim == 0: up to EFM_WAIT_LIMIT polls that may suspend
+// the thread (the default); lim > 0: up to lim polls that do not suspend it -- a limit a
+// failure-detection test sets so short that a wait for a tile still in flight gives up.
+// False when it gave up (error flag set).
 __device__ __forceinline__ bool efm_mbar_wait(uint64_t *bar, uint32_t parity,
                                               unsigned int *err_flag, uint32_t lim = 0) {
     if (lim == 0) {
@@ -68,7 +67,7 @@ __device__ __forceinline__ bool efm_mbar_wait(uint64_t *bar, uint32_t parity,
             if (efm_mbar_try_wait(bar, parity)) return true;
     } else {
         for (uint32_t i = 0; i < lim; ++i)
-            if (efm_mbar_try_wait_ns(bar, parity, EFM_WAIT_HINT_NS)) return true;
+            if (efm_mbar_test_wait(bar, parity)) return true;
     }
     if (err_flag) atomicOr(err_flag, EFM_ERR_FLAG_TIMEOUT);
     return false;

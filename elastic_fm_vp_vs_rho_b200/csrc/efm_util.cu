@@ -160,10 +160,12 @@ __global__ void k_chain(float *__restrict__ gl, float *__restrict__ gm, float *_
                         const float *__restrict__ rho, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const float l = gl[i], m = gm[i], r = rho[i], p = vp[i], s = vs[i];
-        gl[i] = 2.f * r * p * l;
-        gm[i] = 2.f * r * s * (m - 2.f * l);
-        gr[i] = gr[i] + (p * p - 2.f * s * s) * l + s * s * m;
+        // float64 arithmetic: g_mu - 2 g_lambda and the rho sum cancel strongly, and float32
+        // intermediates would add rounding of the large terms to the small results
+        const double l = gl[i], m = gm[i], r = rho[i], p = vp[i], s = vs[i];
+        gl[i] = (float)(2.0 * r * p * l);
+        gm[i] = (float)(2.0 * r * s * (m - 2.0 * l));
+        gr[i] = (float)((double)gr[i] + (p * p - 2.0 * s * s) * l + s * s * m);
     }
 }
 

@@ -19,15 +19,25 @@ model to a model update:
     output:  channels 0-2 = the update direction for (Vp, Vs, rho) in normalised units.
 
 Training pairs come from plain L-BFGS runs on seeded random models: the features of each
-iterate and, as target, either GAIN x (true - current) normalised model ("error", the
-default) or the accepted L-BFGS update scaled to unit maximum ("update"); the loss is the
-mean squared error over the three used channels; Adam on FP32 master weights.
+iterate (raw gradient, model, depth, forward illumination) and, as target, one of
 
-:func:`invert` runs an inversion with either plain L-BFGS or the learned direction; every
-learned direction must pass a descent test (g . d < 0) and an Armijo backtracking line
-search, otherwise that iteration falls back to the plain L-BFGS direction.  Solves are
-counted as in the reference's loop: a gradient costs one forward and one adjoint solve, a
-line-search trial one forward solve.
+* "lbfgs" (default): GAIN x (p_N - p_k), the sum of the accepted L-BFGS updates the plain
+  run itself takes from iterate k to its last iterate N, in normalised units -- where the
+  method ends up, learned from its own accepted steps;
+* "update": the single accepted L-BFGS update of iteration k scaled to unit maximum;
+* "error": GAIN x (true - current) normalised model (the seeded problems know their true
+  model; an upper bound of what a preconditioner could learn, not available in practice);
+
+the loss is the mean squared error over the three used channels; Adam on FP32 master
+weights.
+
+:func:`invert` runs an inversion with either plain L-BFGS (the reference's two-loop
+recursion and history layout, ``lbfgs.compute_sk_yk`` / ``lbfgs.L_BFGS`` on the GPU with
+float64 dot products) or the learned direction.  Every step passes a Wolfe line search
+(sufficient decrease and curvature, each trial a misfit + gradient evaluation); a learned
+direction that fails it within ``learned_tries`` trials falls back to the plain L-BFGS
+direction for that iteration.  Solves are counted as in the reference's loop: a misfit +
+gradient evaluation costs one forward and one adjoint solve.
 """
 from __future__ import annotations
 
@@ -40,7 +50,7 @@ from . import conv3d
 
 WIDTHS = (16, 32, 64, 32, 16)
 NFEAT = 8
-GAIN = 10.0  # "error" targets: network output = GAIN x (normalised true model - current)
+GAIN = 10.0  # "error" / "lbfgs" targets: network output = GAIN x (normalised displacement)
 
 
 # ================================================================================ network
@@ -300,123 +310,135 @@ class InversionProblem:
         return float(((p * self.scale - self.true) / self.true).pow(2).mean().sqrt())
 
 
-class LBFGS:
-    """Standard L-BFGS two-loop recursion on the normalised model (float64 dots, memory m)."""
+def _dot(a, b):
+    """float64 dot product on the GPU (efm_dot), as a host float."""
+    from .engine import dot
+    return float(dot(a.contiguous().reshape(-1), b.contiguous().reshape(-1)))
 
-    def __init__(self, m=5):
-        self.m = m
-        self.s, self.y = [], []
 
-    def update(self, s, y):
+class GpuLBFGS:
+    """Plain L-BFGS: the reference's history layout and two-loop recursion
+    (lbfgs.compute_sk_yk / lbfgs.L_BFGS, lbfgs.py:12-67) on the GPU, float64 dot products,
+    scalars on the device.  ``layers`` = lbfgsLayers (layers - 2 curvature pairs)."""
+
+    def __init__(self, shape, layers=7, device="cuda"):
         import torch
-        sy = float(torch.sum(s.double() * y.double()))
-        if sy <= 1e-30:
-            return
-        self.s.append(s)
-        self.y.append(y)
-        if len(self.s) > self.m:
-            self.s.pop(0)
-            self.y.pop(0)
+        self.L = int(layers)
+        self.sk = torch.zeros((self.L,) + tuple(shape), dtype=torch.float32, device=device)
+        self.yk = torch.zeros_like(self.sk)
+        self.work = torch.empty(4 * self.L + 8, dtype=torch.float64, device=device)
+        self.k = -1  # pushes - 1: curvature pairs held (capped at layers - 2 by the recursion)
+
+    def reset(self):
+        self.sk.zero_()
+        self.yk.zero_()
+        self.k = -1
+
+    def push(self, p, g):
+        """compute_sk_yk with the current model and gradient."""
+        from .lbfgs import compute_sk_yk
+        self.k += 1
+        compute_sk_yk(self.sk, self.yk, p.contiguous(), g.contiguous(), self.L, self.k)
+
+    @property
+    def has_pairs(self):
+        return self.k >= 1
 
     def direction(self, g):
-        import torch
-        q = g.clone()
-        al = []
-        for s, y in zip(reversed(self.s), reversed(self.y)):
-            rho = 1.0 / float(torch.sum(y.double() * s.double()))
-            a = rho * float(torch.sum(s.double() * q.double()))
-            q -= a * y
-            al.append((a, rho, s, y))
-        if self.s:
-            s, y = self.s[-1], self.y[-1]
-            q *= float(torch.sum(s.double() * y.double()) / torch.sum(y.double() * y.double()))
-        for a, rho, s, y in reversed(al):
-            b = rho * float(torch.sum(y.double() * q.double()))
-            q += (a - b) * s
-        return -q
+        """-H g from the held pairs, or -g without any."""
+        from .lbfgs import L_BFGS
+        if not self.has_pairs:
+            return -g
+        return -L_BFGS(self.sk, self.yk, g.contiguous(), self.L, self.k, work=self.work)
 
 
-def _line_search(prob, p, J, g, d, alpha0, tries=6, c1=1e-4):
-    """Armijo backtracking; returns (alpha, J_new) or (None, J)."""
-    import torch
-    gd = float(torch.sum(g.double() * d.double()))
+def _wolfe(prob, p, J, g, d, a0, tries=6, c1=1e-4, c2=0.9):
+    """Wolfe line search along d from p (misfit J, gradient g): sufficient decrease
+    J(a) <= J + c1 a g.d and curvature g(a).d >= c2 g.d, bracketing by halving / doubling.
+    Every trial is a misfit + gradient evaluation (2 solves).  Returns (a, J(a), g(a)), the
+    last trial that passed sufficient decrease when none passed both, or None."""
+    gd = _dot(g, d)
     if not gd < 0:
-        return None, J
-    a = alpha0
+        return None
+    lo, hi, a = 0.0, math.inf, a0
+    best = None
     for _ in range(tries):
-        Jn = prob.misfit(p + a * d)
-        if math.isfinite(Jn) and Jn <= J + c1 * a * gd:
-            return a, Jn
-        a *= 0.5
-    return None, J
+        Jn, gn = prob.gradient(p + a * d)
+        if not math.isfinite(Jn) or Jn > J + c1 * a * gd:
+            hi = a
+            a = 0.5 * (lo + hi)
+        elif _dot(gn, d) < c2 * gd:
+            best = (a, Jn, gn)
+            lo = a
+            a = 2.0 * a if math.isinf(hi) else 0.5 * (lo + hi)
+        else:
+            return a, Jn, gn
+    return best
 
 
-def invert(prob, iters, net=None, first_step=0.02, record=None, target="error", log=None,
-           learned_iters=None, learned_tries=2):
+def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", log=None,
+           learned_iters=None, learned_tries=2, layers=7):
     """Plain (net=None) or learned-direction inversion.  Returns a history of dicts
     (iteration, solves so far, misfit, model error, direction used).
 
-    `record`, when a list, receives one training pair per iteration: the features and, for
-    target "error", GAIN x (true model - current model) in normalised units (the update a
-    perfect preconditioner would take; the seeded problems know their true model), or, for
-    target "update", the accepted L-BFGS update scaled to unit maximum.  A network trained
-    on "error" targets proposes its output / GAIN with a unit first trial step; one trained
-    on "update" targets is scaled to the length of the previous accepted step.
+    `record`, when a list, receives one training pair per iteration once the run has ended:
+    the features of iterate k and its target (see the module docstring: "lbfgs", "update"
+    or "error").  A network proposes its output / GAIN with a unit first trial step.
 
     learned_iters: use the network only in the first that many iterations (None: always);
-    learned_tries: line-search trials a learned direction gets before the iteration falls
-    back to L-BFGS."""
-    import torch
+    learned_tries: Wolfe trials a learned direction gets before the iteration falls back to
+    L-BFGS."""
     p = (prob.init / prob.scale).contiguous()
-    lb = LBFGS(5)
+    lb = GpuLBFGS(p.shape, layers)
     prob.solves = 0
     J, g = prob.gradient(p)
     hist = [dict(it=0, solves=prob.solves, misfit=J, model_error=prob.model_error(p), used="init")]
-    last_step = first_step
+    kept = []
     for it in range(1, iters + 1):
-        used = None
-        step = None
-        if net is not None and (learned_iters is None or it <= learned_iters):
+        lb.push(p, g)
+        use_net = net is not None and (learned_iters is None or it <= learned_iters)
+        acc, used, d = None, None, None
+        if use_net:
             out = net.forward(features(g, p, prob.illum))
-            d = out[..., :3].permute(3, 0, 1, 2).contiguous()
-            dmax = float(d.abs().max())
-            if net.target == "error":
-                d /= GAIN
-                a0 = 1.0
-            else:
-                a0 = last_step / max(dmax, 1e-30)
-            if dmax > 0:
-                a, Jn = _line_search(prob, p, J, g, d, a0, tries=learned_tries)
-                if a is not None:
-                    step, used = a * d, "learned"
-        if step is None:
+            d = (out[..., :3].permute(3, 0, 1, 2) / GAIN).contiguous()
+            if float(d.abs().max()) > 0:
+                acc = _wolfe(prob, p, J, g, d, 1.0, tries=learned_tries)
+                used = "learned"
+        if acc is None:
             d = lb.direction(g)
-            a0 = 1.0 if lb.s else first_step / max(float(d.abs().max()), 1e-30)
-            a, Jn = _line_search(prob, p, J, g, d, a0)
-            if a is None and lb.s:
+            a0 = 1.0 if lb.has_pairs else first_step / max(float(d.abs().max()), 1e-30)
+            acc = _wolfe(prob, p, J, g, d, a0)
+            if acc is None and lb.has_pairs:
                 # restart: drop the curvature pairs, retry along the steepest descent
-                lb = LBFGS(lb.m)
+                lb.reset()
+                lb.push(p, g)
                 d = -g
-                a, Jn = _line_search(prob, p, J, g, d, first_step / max(float(d.abs().max()), 1e-30))
-            if a is None:
+                acc = _wolfe(prob, p, J, g, d, first_step / max(float(d.abs().max()), 1e-30))
+            if acc is None:
                 hist.append(dict(it=it, solves=prob.solves, misfit=J,
                                  model_error=prob.model_error(p), used="stalled"))
                 break
-            step, used = a * d, ("fallback" if net is not None and (
-                learned_iters is None or it <= learned_iters) else "lbfgs")
+            used = "fallback" if use_net else "lbfgs"
+        a, J_new, g_new = acc
+        step = a * d
         if record is not None:
-            t = ((prob.true / prob.scale - p) * GAIN if target == "error"
-                 else step / step.abs().max())
-            record.append((features(g, p, prob.illum), t.permute(1, 2, 3, 0).contiguous()))
-        p_new = p + step
-        J_new, g_new = prob.gradient(p_new)
-        lb.update(step, g_new - g)
-        last_step = float(step.abs().max())
-        p, J, g = p_new, J_new, g_new
+            kept.append((features(g, p, prob.illum), p.clone(), step / step.abs().max()))
+        if _dot(step, g_new - g) <= 0:
+            lb.reset()  # no curvature along this step (curvature test waived): start afresh
+        p, J, g = (p + step).contiguous(), J_new, g_new
         hist.append(dict(it=it, solves=prob.solves, misfit=J, model_error=prob.model_error(p),
                          used=used))
         if log:
             log(f"it {it}: J {J:.4e} solves {prob.solves} ({used})")
+    if record is not None:
+        for f, pk, unit_step in kept:
+            if target == "error":
+                t = (prob.true / prob.scale - pk) * GAIN
+            elif target == "lbfgs":
+                t = (p - pk) * GAIN
+            else:
+                t = unit_step
+            record.append((f, t.permute(1, 2, 3, 0).contiguous()))
     return hist
 
 
@@ -432,7 +454,7 @@ POLICIES = {"always": dict(learned_iters=None), "first2": dict(learned_iters=2),
 
 
 def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=12, epochs=40,
-               spec=None, target="error", log=None, illumination=False):
+               spec=None, target="lbfgs", log=None, illumination=True, policies=None):
     """Train on plain-L-BFGS runs of seeded models, then, on unseen seeds, compare plain
     L-BFGS with each learned policy: the solves each needs to reach plain L-BFGS's final
     misfit (None: not reached within `iters` iterations)."""
@@ -456,7 +478,7 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
         target_j = plain[-1]["misfit"]
         row = dict(seed=ts, target_misfit=target_j, solves_plain=plain[-1]["solves"],
                    plain=plain, policies={})
-        for name, kw in POLICIES.items():
+        for name, kw in (policies or POLICIES).items():
             h = invert(prob, iters, net=net, log=log, **kw)
             row["policies"][name] = dict(solves=solves_to_reach(h, target_j),
                                          final_misfit=h[-1]["misfit"],
@@ -465,7 +487,7 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
         prob.batch.close()
         tests.append(row)
     summary = {}
-    for name in POLICIES:
+    for name in (policies or POLICIES):
         r = [t["solves_plain"] / t["policies"][name]["solves"] if t["policies"][name]["solves"]
              else 0.0 for t in tests]
         summary[name] = dict(solve_ratio_per_seed=r, reached=sum(x > 0 for x in r))
@@ -483,22 +505,28 @@ if __name__ == "__main__":
     ap.add_argument("--iters", type=int, default=12)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--train", type=int, default=8, help="number of training seeds")
-    ap.add_argument("--target", default="error", choices=["error", "update"])
+    ap.add_argument("--target", default="lbfgs", choices=["lbfgs", "update", "error"])
     ap.add_argument("--test-seeds", default="7,8,9")
     ap.add_argument("--grid", default="48,48,40", help="nx,ny,nz")
     ap.add_argument("--nt", type=int, default=320)
     ap.add_argument("--shots", type=int, default=4)
     ap.add_argument("--receivers", type=int, default=8, help="per side of the surface grid")
-    ap.add_argument("--illumination", action="store_true",
-                    help="fill feature channel 7 with the forward illumination")
+    ap.add_argument("--no-illumination", action="store_true",
+                    help="leave feature channel 7 (forward illumination) empty")
+    ap.add_argument("--dx", type=float, default=10.0)
+    ap.add_argument("--lenpml", type=int, default=8)
+    ap.add_argument("--fq", type=float, default=12.0)
+    ap.add_argument("--policies", default="first2,always", help="comma list of " + ",".join(POLICIES))
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
     gx, gy, gz = (int(v) for v in a.grid.split(","))
-    spec = ProblemSpec(nx=gx, ny=gy, nz=gz, nt=a.nt, nshots=a.shots, nrec=a.receivers)
+    spec = ProblemSpec(nx=gx, ny=gy, nz=gz, nt=a.nt, nshots=a.shots, nrec=a.receivers, dx=a.dx,
+                       lenpml=a.lenpml, fq=a.fq)
     r = experiment(train_seeds=tuple(range(100, 100 + a.train)),
                    test_seeds=tuple(int(v) for v in a.test_seeds.split(",")),
                    iters=a.iters, epochs=a.epochs, spec=spec, target=a.target, log=print,
-                   illumination=a.illumination)
+                   illumination=not a.no_illumination,
+                   policies={k: POLICIES[k] for k in a.policies.split(",")})
     s = json.dumps(r, indent=1)
     if a.out:
         with open(a.out, "w") as f:

@@ -223,8 +223,10 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
  * the same (kernel counters still count every launch); 0: launched step by step.  Loops
  * run with efm_set_timing(ctx, 1) are always launched step by step. */
 #define EFM_OPT_GRAPH 8
-/* Bound of every tile wait of the plane-streaming kernels: 0 (default) = 2^22 polls; n > 0 =
- * n polls of about 32 ns each.  A wait that runs out sets the context's error word
+/* Bound of every tile wait of the plane-streaming kernels: 0 (default) = 2^22 polls that may
+ * suspend the thread; n > 0 = n polls that do not (a few ns each, shorter than a tile load's
+ * latency, so n = 1 gives up on a tile still in flight).  A wait that runs out sets the
+ * context's error word
  * (efm_status -> EFM_ERR_TIMEOUT), waits for its block's own loads still in flight and
  * returns; the call completes with invalid outputs, and the next call with the default
  * limit is unaffected.  Small values exist for failure-detection tests (no reference

@@ -59,14 +59,16 @@ def test_learned_inversion_with_fallback(cuda):
     from elastic_fm_vp_vs_rho_b200.precond import (InversionProblem, PreconditionerNet,
                                                    ProblemSpec, invert, train)
     spec = ProblemSpec(nx=32, ny=32, nz=28, lenpml=6, nt=200, nshots=2, nrec=6, seed=11)
-    prob = InversionProblem(spec)
+    prob = InversionProblem(spec, illumination=True)
     samples = []
     plain = invert(prob, 3, record=samples)
     assert len(samples) == 3
     Js = [h["misfit"] for h in plain]
     assert all(b < a for a, b in zip(Js, Js[1:]))
-    # every iteration: >= one line-search forward + one forward/adjoint gradient
-    assert all(b["solves"] - a["solves"] >= 3 for a, b in zip(plain, plain[1:]))
+    # every iteration: at least one Wolfe trial = one forward + one adjoint solve
+    assert all(b["solves"] - a["solves"] >= 2 for a, b in zip(plain, plain[1:]))
+    assert all(h["used"] == "lbfgs" for h in plain[1:])
+    assert float(samples[0][0][..., 7].float().max()) == 1.0  # illumination channel filled
     net = PreconditionerNet(seed=0)
     losses = train(net, samples, epochs=6)
     assert losses[-1] < losses[0]
@@ -76,29 +78,30 @@ def test_learned_inversion_with_fallback(cuda):
     assert all(h["used"] in ("learned", "fallback") for h in learned[1:])
 
 
-def test_lbfgs_recursion_solves_a_quadratic():
-    """CPU: the two-loop recursion with exact line minimisation converges on a quadratic."""
+@pytest.mark.gpu
+def test_gpu_lbfgs_solves_a_quadratic(cuda):
+    """The reference's two-loop recursion (GPU, float64 dots) with exact line minimisation
+    converges on a convex quadratic."""
     import torch
-    from elastic_fm_vp_vs_rho_b200.precond import LBFGS
+    from elastic_fm_vp_vs_rho_b200.precond import GpuLBFGS
     rng = np.random.default_rng(0)
     n = 12
     Q = rng.standard_normal((n, n))
-    A = torch.as_tensor(Q @ Q.T + n * np.eye(n))
-    b = torch.as_tensor(rng.standard_normal(n))
+    A = torch.as_tensor(Q @ Q.T + n * np.eye(n), dtype=torch.float64)
+    b = torch.as_tensor(rng.standard_normal(n), dtype=torch.float64)
     x = torch.zeros(n, dtype=torch.float64)
-    lb = LBFGS(m=n)
+    lb = GpuLBFGS((n,), layers=n + 2)
     g = A @ x - b
+    g0 = float(g.norm())
     for _ in range(2 * n):
-        d = lb.direction(g)
+        lb.push(x.float().cuda(), g.float().cuda())
+        d = lb.direction(g.float().cuda()).double().cpu()
         a = -float(g @ d) / float(d @ A @ d)
-        s = a * d
-        x = x + s
-        gn = A @ x - b
-        lb.update(s, gn - g)
-        g = gn
-        if float(g.norm()) < 1e-10:
+        x = x + a * d
+        g = A @ x - b
+        if float(g.norm()) < 1e-5 * g0:
             break
-    assert float(g.norm()) < 1e-8
+    assert float(g.norm()) < 1e-4 * g0
 
 
 def test_network_state_and_adam_on_cpu():

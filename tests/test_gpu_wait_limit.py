@@ -1,7 +1,8 @@
 """Failure detection on the GPU: a tile wait that runs out ends in an error status.
 
 Every mbarrier wait of the plane-streaming kernels is bounded.  With EFM_OPT_WAIT_LIMIT set
-to one poll of ~32 ns, a wait for a tile that is still in flight gives up: the kernel sets
+to one poll that does not suspend the thread, a wait for a tile that is still in flight
+(the first tiles of every block are issued just before it) gives up: the kernel sets
 the context's error word, waits (with the default bound) for its own loads still in
 flight, and returns, so the call completes and efm_status reports EFM_ERR_TIMEOUT.  The
 next call with the default limit must give bit-identical results to a run that never

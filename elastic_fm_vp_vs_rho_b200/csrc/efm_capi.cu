@@ -157,6 +157,7 @@ struct efm_ctx {
     int ring = 4;  // ring depth of those tables' kernels
     int opt_ck_every = 50;
     unsigned int opt_wait = 0;  // polls per tile wait (0: the kernels' default bound)
+    int opt_exact_fused = 1;    // exact adjoint: one gather launch per transposed half-step
     // kernel kinds whose device tables (and tensor maps) are loaded now, for efm_kernel_time,
     // and the step count of those tables
     unsigned int timeable = 0;
@@ -805,12 +806,13 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
                      return efm_launch_exact(0, t, n, 0, it, slot, s);
                  })))
                 return rc;
+            const int kv = ctx->opt_exact_fused ? 4 : 1, ks = ctx->opt_exact_fused ? 5 : 2;
             if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
-                     return efm_launch_exact(1, t, n, tiles, it, slot, s);
+                     return efm_launch_exact(kv, t, n, tiles, it, slot, s);
                  })))
                 return rc;
             if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
-                     return efm_launch_exact(2, t, n, tiles, it, slot, s);
+                     return efm_launch_exact(ks, t, n, tiles, it, slot, s);
                  })))
                 return rc;
             parity ^= 1;
@@ -1408,6 +1410,7 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             if (value != 0 && value != 4 && value != 6) return fail(EFM_ERR_ARG, "ring depth must be 0, 4 or 6");
             ctx->opt_ring = value;
             break;
+        case EFM_OPT_EXACT_FUSED: ctx->opt_exact_fused = value != 0; break;
         case EFM_OPT_WAIT_LIMIT:
             if (value < 0) return fail(EFM_ERR_ARG, "wait limit must be >= 0 (0 = default)");
             ctx->opt_wait = (unsigned int)value;

@@ -323,12 +323,198 @@ efm_exact_stress_T_gather(const EfmExact *__restrict__ t, int n, int step, int s
     I.g_mu[p] += acc * f;
 }
 
+// ---------------------------------------------------------------- fused transposed half-steps
+// The same arithmetic as the cells + gather pairs above, in one pass per half-step: each
+// thread recomputes the gbar / dbar values of the neighbours it gathers (and the shear
+// products of the mu gradient) from the adjoint fields, instead of reading them from scratch
+// volumes another launch wrote.  Every value is formed by the same expressions as in the
+// cells passes, so the results match those of the two-launch form.
+
+// gbar_kk of the velocity transpose at cell (cx, cy, cz); zero outside the update domain
+__device__ __forceinline__ float gbar_at(const G &g, int kk, int cx, int cy, int cz) {
+    if (!g.in(cx, cy, cz)) return 0.f;
+    const EfmExact &I = g.I;
+    const int i = vt_comp(kk), d = vt_family(kk);
+    const int64_t c = g.lin(cx, cy, cz);
+    const float ub = I.k * g.buoy_avg(i, cx, cy, cz) * I.bv[i][c];
+    const int q = d == 0 ? cx : (d == 1 ? cy : cz);
+    const float a = g.a(d, q);
+    return a == 0.f ? ub : (1.f + a) * ub + a * g.psi_in(d, 3 + kk % 3, cx, cy, cz);
+}
+
+// e_kk of the stress transpose at cell (cx, cy, cz) (the entries of ebar_all)
+__device__ __forceinline__ float ebar_at(const G &g, int kk, int cx, int cy, int cz) {
+    const EfmExact &I = g.I;
+    const int64_t c = g.lin(cx, cy, cz);
+    const float k = I.k;
+    if (kk == 0 || kk == 3 || kk == 6) {
+        const float lam = I.lam[c], mu = I.mu[c];
+        const float txx = I.bt[0][c], tyy = I.bt[1][c], tzz = I.bt[2][c];
+        if (kk == 0) return k * ((lam + 2.f * mu) * txx + lam * tyy + lam * tzz);
+        if (kk == 3) return k * (lam * txx + (lam + 2.f * mu) * tyy + lam * tzz);
+        return k * (lam * txx + lam * tyy + (lam + 2.f * mu) * tzz);
+    }
+    if (kk == 1 || kk == 4) return k * g.mu_avg(0, cx, cy, cz) * I.bt[3][c];
+    if (kk == 2 || kk == 7) return k * g.mu_avg(1, cx, cy, cz) * I.bt[4][c];
+    return k * g.mu_avg(2, cx, cy, cz) * I.bt[5][c];
+}
+
+// dbar_kk of the stress transpose at cell (cx, cy, cz); zero outside the update domain
+__device__ __forceinline__ float dbar_at(const G &g, int kk, int cx, int cy, int cz) {
+    if (!g.in(cx, cy, cz)) return 0.f;
+    const int d = kk / 3;
+    const int q = d == 0 ? cx : (d == 1 ? cy : cz);
+    const float a = g.a(d, q);
+    const float e = ebar_at(g, kk, cx, cy, cz);
+    return a == 0.f ? e : (1.f + a) * e + a * g.psi_in(d, kk % 3, cx, cy, cz);
+}
+
+// stress increment of step n at a cell, without the source
+__device__ __forceinline__ float dtau_at(const EfmExact &I, const float *tn, const float *tm,
+                                         int64_t N, int comp, int64_t c, int x, int y, int z,
+                                         int step) {
+    float d = tn[comp * N + c] - tm[comp * N + c];
+    for (int s = 0; s < I.nsrc; ++s)
+        if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s]) d -= I.mt[s][comp] * I.wav[step];
+    return d;
+}
+
+// shear product taubar_ij * dtau_ij * mu_ij of the stress transpose at a cell (zero outside
+// the update domain)
+__device__ __forceinline__ float shear_at(const G &g, const float *tn, const float *tm, int64_t N,
+                                          int pair, int cx, int cy, int cz, int step) {
+    if (!g.in(cx, cy, cz)) return 0.f;
+    const int64_t c = g.lin(cx, cy, cz);
+    return g.I.bt[3 + pair][c] * dtau_at(g.I, tn, tm, N, 3 + pair, c, cx, cy, cz, step) *
+           g.mu_avg(pair, cx, cy, cz);
+}
+
+__global__ void __launch_bounds__(EFM_THREADS)
+efm_exact_velocity_T(const EfmExact *__restrict__ t, int n, int step, int slot) {
+    const EfmExact &I = find(t, n, blockIdx.x);
+    int x, y, z;
+    if (!cell_of(I, x, y, z)) return;
+    G g(I);
+    const int64_t p = g.lin(x, y, z);
+    const int64_t N = I.slot_stride / 9;
+    if (g.in(x, y, z)) {
+        float ub[3];
+        for (int i = 0; i < 3; ++i) ub[i] = I.k * g.buoy_avg(i, x, y, z) * I.bv[i][p];
+        // memory variables of the velocity update: psibar <- b (psibar + ubar)
+#pragma unroll
+        for (int kk = 0; kk < 9; ++kk) {
+            const int i = vt_comp(kk), d = vt_family(kk);
+            const int q = d == 0 ? x : (d == 1 ? y : z);
+            const int64_t ix = g.psi_idx(d, 3 + kk % 3, x, y, z);
+            if (ix >= 0) I.pout[ix] = g.b(d, q) * (I.pin[ix] + ub[i]);
+        }
+        // taubar += D_T^T gbar
+        const float g0 = gbar_at(g, 0, x, y, z), g3 = gbar_at(g, 3, x, y, z);
+        const float g6 = gbar_at(g, 6, x, y, z), g4 = gbar_at(g, 4, x, y, z);
+        const float g1 = gbar_at(g, 1, x, y, z), g7 = gbar_at(g, 7, x, y, z);
+        const float g2 = gbar_at(g, 2, x, y, z), g8 = gbar_at(g, 8, x, y, z);
+        const float g5 = gbar_at(g, 5, x, y, z);
+        I.bt[0][p] += gbar_at(g, 0, x - 1, y, z) - g0;
+        I.bt[1][p] += gbar_at(g, 3, x, y - 1, z) - g3;
+        I.bt[2][p] += gbar_at(g, 6, x, y, z - 1) - g6;
+        I.bt[3][p] += g4 - gbar_at(g, 4, x, y + 1, z) + g1 - gbar_at(g, 1, x + 1, y, z);
+        I.bt[4][p] += g7 - gbar_at(g, 7, x, y, z + 1) + g2 - gbar_at(g, 2, x + 1, y, z);
+        I.bt[5][p] += g8 - gbar_at(g, 8, x, y, z + 1) + g5 - gbar_at(g, 5, x, y + 1, z);
+    }
+    // rho gradient: -1/2 sum_i B_i(c) vbar_i(c) dv_i(c) over c in {p, p - e_i} that are updated
+    const float *vn = I.seg + (int64_t)slot * I.slot_stride;
+    const float *vm = vn - I.slot_stride;
+    float acc = 0.f;
+    const int64_t e[3] = {1, g.SY, g.SZ};
+    const int dx_[3] = {1, 0, 0}, dy_[3] = {0, 1, 0}, dz_[3] = {0, 0, 1};
+    for (int i = 0; i < 3; ++i) {
+        for (int s = 0; s < 2; ++s) {
+            const int cx = x - s * dx_[i], cy = y - s * dy_[i], cz = z - s * dz_[i];
+            if (!g.in(cx, cy, cz)) continue;
+            const int64_t c = p - s * e[i];
+            const float B = g.buoy_avg(i, cx, cy, cz);
+            acc += B * I.bv[i][c] * (vn[i * N + c] - vm[i * N + c]);
+        }
+    }
+    I.g_rho[p] += -0.5f * acc;
+}
+
+__global__ void __launch_bounds__(EFM_THREADS)
+efm_exact_stress_T(const EfmExact *__restrict__ t, int n, int step, int slot) {
+    const EfmExact &I = find(t, n, blockIdx.x);
+    int x, y, z;
+    if (!cell_of(I, x, y, z)) return;
+    G g(I);
+    const int64_t p = g.lin(x, y, z);
+    const float *tn = I.seg + (int64_t)slot * I.slot_stride + 3 * (I.slot_stride / 9);
+    const float *tm = tn - I.slot_stride;
+    const int64_t N = I.slot_stride / 9;
+    if (g.in(x, y, z)) {
+        // MT gradient at the source cell: Mbar += w[n] taubar(src)
+        if (I.mtg != nullptr)
+            for (int s = 0; s < I.nsrc; ++s)
+                if (x == I.sx[s] && y == I.sy[s] && z == I.sz[s])
+                    for (int c6 = 0; c6 < 6; ++c6)
+                        I.mtg[6 * s + c6] += (double)I.wav[step] * (double)I.bt[c6][p];
+        float e[9];
+        ebar_all(g, x, y, z, e);
+#pragma unroll
+        for (int kk = 0; kk < 9; ++kk) {
+            const int d = kk / 3;
+            const int q = d == 0 ? x : (d == 1 ? y : z);
+            const int64_t ix = g.psi_idx(d, kk % 3, x, y, z);
+            if (ix >= 0) I.pout[ix] = g.b(d, q) * (I.pin[ix] + e[kk]);
+        }
+        // lambda and diagonal mu terms
+        const float lam = I.lam[p], mu = I.mu[p];
+        const float b0 = I.bt[0][p], b1 = I.bt[1][p], b2 = I.bt[2][p];
+        const float d0 = dtau_at(I, tn, tm, N, 0, p, x, y, z, step);
+        const float d1 = dtau_at(I, tn, tm, N, 1, p, x, y, z, step);
+        const float d2 = dtau_at(I, tn, tm, N, 2, p, x, y, z, step);
+        const float sb = b0 + b1 + b2, sd = d0 + d1 + d2;
+        const float inv = 1.f / (3.f * lam + 2.f * mu);
+        I.g_lam[p] += sb * sd * inv;
+        I.g_mu[p] += (b0 * d0 + b1 * d1 + b2 * d2 - lam * sb * sd * inv) / mu;
+        // vbar += D_V^T dbar
+        const float q0 = dbar_at(g, 0, x, y, z), q7 = dbar_at(g, 7, x, y, z);
+        const float q4 = dbar_at(g, 4, x, y, z), q3 = dbar_at(g, 3, x, y, z);
+        const float q1 = dbar_at(g, 1, x, y, z), q8 = dbar_at(g, 8, x, y, z);
+        const float q6 = dbar_at(g, 6, x, y, z), q2 = dbar_at(g, 2, x, y, z);
+        const float q5 = dbar_at(g, 5, x, y, z);
+        I.bv[0][p] += q0 - dbar_at(g, 0, x + 1, y, z) + dbar_at(g, 7, x, y, z - 1) - q7 +
+                      dbar_at(g, 4, x, y - 1, z) - q4;
+        I.bv[1][p] += q3 - dbar_at(g, 3, x, y + 1, z) + dbar_at(g, 1, x - 1, y, z) - q1 +
+                      dbar_at(g, 8, x, y, z - 1) - q8;
+        I.bv[2][p] += q6 - dbar_at(g, 6, x, y, z + 1) + dbar_at(g, 2, x - 1, y, z) - q2 +
+                      dbar_at(g, 5, x, y - 1, z) - q5;
+    }
+    // shear mu terms: mu(p) enters mu_xy, mu_xz, mu_yz of up to four updated cells each
+    const float mup = I.mu[p];
+    const float f = 0.25f / (mup * mup);
+    float acc = 0.f;
+#pragma unroll
+    for (int pair = 0; pair < 3; ++pair) {
+        // first axis: x for xy/xz, y for yz; second axis: y for xy, z for xz/yz
+        const int ax1 = pair == 2 ? 1 : 0, ax2 = pair == 0 ? 1 : 2;
+        const int x1 = x - (ax1 == 0), y1 = y - (ax1 == 1);
+        const int x2 = x, y2 = y - (ax2 == 1), z2 = z - (ax2 == 2);
+        acc += shear_at(g, tn, tm, N, pair, x, y, z, step) + shear_at(g, tn, tm, N, pair, x1, y1, z, step) +
+               shear_at(g, tn, tm, N, pair, x2, y2, z2, step) +
+               shear_at(g, tn, tm, N, pair, x1, y2 - (y - y1), z2, step);
+    }
+    I.g_mu[p] += acc * f;
+}
+
 extern "C" cudaError_t efm_launch_exact(int kind, const EfmExact *t, int n, int tiles, int step,
                                         int slot, cudaStream_t s) {
     if (kind == 3) {
         efm_exact_averages<<<tiles, EFM_THREADS, 0, s>>>(t, n);
     } else if (kind == 0) {
         efm_exact_inject<<<n, EFM_THREADS, 0, s>>>(t, n, step);
+    } else if (kind == 4) {
+        efm_exact_velocity_T<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
+    } else if (kind == 5) {
+        efm_exact_stress_T<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
     } else if (kind == 1) {
         efm_exact_velocity_T_cells<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);
         efm_exact_velocity_T_gather<<<tiles, EFM_THREADS, 0, s>>>(t, n, step, slot);

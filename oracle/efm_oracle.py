@@ -233,12 +233,22 @@ def velocity_step(st: State, md: Model, cp, dt: float, dx: float):
     st.vz[c] += k * md.b_z * ((dtxz_dx + p3) + (dtyz_dy + p6) + (dtzz_dz + p7))
 
 
+def _sources(src, mt):
+    """One (x, y, z) cell and 6 MT components, or several of each (an instance with
+    several sources: rows of src and mt) -> list of (cell, MT) pairs."""
+    cells = np.asarray(src, np.int64).reshape(-1, 3)
+    mts = np.asarray(mt, np.float64).reshape(-1, 6)
+    if len(cells) != len(mts):
+        raise ValueError("one moment tensor per source")
+    return [(tuple(int(v) for v in c), m) for c, m in zip(cells, mts)]
+
+
 def add_source(st: State, src, mt, w_it: float, sign: float = 1.0):
     """Elastic3D.addSource (:1728-1734): tau_ij(Sy, Sz, Sx) += sign * M_ij * w[it]
-    (no dt or volume scaling)."""
-    sx, sy, sz = src
-    for name, m in zip(FIELDS_T, mt):
-        getattr(st, name)[sy, sz, sx] += sign * float(np.float32(m)) * float(w_it)
+    (no dt or volume scaling); with several sources each one in turn."""
+    for (sx, sy, sz), m6 in _sources(src, mt):
+        for name, m in zip(FIELDS_T, m6):
+            getattr(st, name)[sy, sz, sx] += sign * float(np.float32(m)) * float(w_it)
 
 
 def record(st: State, rec):
@@ -384,18 +394,21 @@ def _inject(bst: State, rec, res, it_res):
 def mt_gradient(lam, mu, rho, cp, wavelet, dt, dx, src, rec, res):
     """Elastic3D.backwardFields with mode 0 (:2056-2082): for it in 0..nt-1, adjoint
     tau and v steps (+dt, same operator as the forward), inject res[nt-1-it] into v,
-    then g_k += w[nt-1-it] * strain_k(adjoint tau at the source)."""
+    then g_k += w[nt-1-it] * strain_k(adjoint tau at the source).  With several source
+    cells (rows of src) the strain of each, (nsrc, 6); else (6,)."""
     md = Model(lam, mu, rho)
     ny, nz, nx = md.lam.shape
     bst = State(ny, nz, nx)
     nt = len(wavelet)
-    g = np.zeros(6)
+    cells = np.asarray(src, np.int64).reshape(-1, 3)
+    g = np.zeros((len(cells), 6))
     for it in range(nt):
         stress_step(bst, md, cp, dt, dx)
         velocity_step(bst, md, cp, dt, dx)
         _inject(bst, rec, res, nt - it - 1)
-        g += float(wavelet[nt - it - 1]) * _mt_strain(md, bst, src)
-    return g
+        for q, c in enumerate(cells):
+            g[q] += float(wavelet[nt - it - 1]) * _mt_strain(md, bst, tuple(int(v) for v in c))
+    return g if np.asarray(src).ndim > 1 else g[0]
 
 
 def imaging_terms(md: Model, bst: State, fv_prev, fv, dt, dx):
@@ -482,7 +495,7 @@ def gradient_reference(lam, mu, rho, cp, wavelet, dt, dx, src, mt, rec, obs, wid
         g_lam[c] += l
         g_mu[c] += m
         if want_mt:
-            g_mt += float(wavelet[nt - it - 1]) * _mt_strain(md, bst, src)
+            g_mt += float(wavelet[nt - it - 1]) * _mt_strain(md, bst, _sources(src, mt)[0][0])
     out = dict(gathers=gathers, res=res, misfit=J, g_lam=g_lam, g_mu=g_mu, g_rho=g_rho)
     if want_mt:
         out["g_mt"] = g_mt

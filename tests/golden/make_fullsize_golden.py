@@ -17,6 +17,8 @@ Run where the reference tree is present (it is read-only and never shipped)::
   ``oracle/ref_driver.py`` (the reference's kernels in its per-step order, several
   sources per step): misfit, lambda/mu/rho gradient from the model smoothed with
   sigma = 3 cells, MT gradient of every source from a perturbed MT.
+* ``c4fp64`` -- the same six instances through the FP64 NumPy oracle (``efm_oracle``),
+  end to end in float64, summarised on the cells ``c4inst`` samples.
 
 Volumes and large gathers are stored as summaries (``fullsize.py``: sampled cells + norm
 and projections); scalars, wavelets, CPML profiles and geometry whole.  Models are not
@@ -157,11 +159,52 @@ def run_c4():
     np.savez_compressed(os.path.join(HERE, "c4inst.npz"), **out)
 
 
+def _c4_fp64_one(k):
+    """FP64 oracle (efm_oracle) on uneven instance k, end to end: observed data, misfit and
+    imaging gradient from the starting model, MT gradient of every source."""
+    import efm_oracle as O
+    c = c4_instance_inputs(k)
+    inst = c["inst"]
+    rec = (inst.rec[:, 0], inst.rec[:, 1], inst.rec[:, 2])
+    t0 = time.time()
+    obs = O.forward(c["lam"], c["mu"], c["rho"], c["cp"], c["wav"], inst.dt, inst.dx, inst.src,
+                    c["mt_obs"], rec)
+    r = O.gradient_reference(c["lam0"], c["mu0"], c["rho0"], c["cp"], c["wav"], inst.dt, inst.dx,
+                             inst.src, c["mt_obs"], rec, obs, width=inst.lenpml)
+    gm = O.forward(c["lam"], c["mu"], c["rho"], c["cp"], c["wav"], inst.dt, inst.dx, inst.src,
+                   c["mt_mod"], rec)
+    resm, mism = O.misfit(gm, obs)
+    gmt = O.mt_gradient(c["lam"], c["mu"], c["rho"], c["cp"], c["wav"], inst.dt, inst.dx,
+                        inst.src, rec, resm)
+    return k, r, float(mism), np.asarray(gmt).reshape(-1, 6), time.time() - t0
+
+
+def run_c4_fp64():
+    """c4fp64.npz: the FP64 oracle's summaries of the same sampled cells as c4inst.npz."""
+    import multiprocessing as mp
+    ref = dict(np.load(os.path.join(HERE, "c4inst.npz")))
+    out = {"pick": np.array(C4_PICK, np.int32)}
+    with mp.get_context("spawn").Pool(len(C4_PICK)) as pool:
+        for k, r, mism, gmt, secs in pool.imap_unordered(_c4_fp64_one, C4_PICK):
+            p = f"i{k}_"
+            idx = ref[p + "index"].astype(np.int64)
+            out[p + "misfit"] = np.float64(r["misfit"])
+            out[p + "mt_misfit"] = np.float64(mism)
+            out[p + "g_mt"] = gmt
+            for name in ("g_lam", "g_mu", "g_rho"):
+                out.update(fullsize.pack_volume(p + name, r[name], idx))
+            out[p + "fp64_seconds"] = np.float64(secs)
+            print(f"c4 instance {k}: FP64 oracle {secs:.0f} s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "c4fp64.npz"), **out)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["c1", "c2", "c4"]
+    which = sys.argv[1:] or ["c1", "c2", "c4", "c4fp64"]
     if "c1" in which:
         run_harness_case("c1full", c1_inputs(), n_random=16384, stride=2)
     if "c2" in which:
         run_harness_case("c2full", c2_inputs(), n_random=32768, stride=16)
     if "c4" in which:
         run_c4()
+    if "c4fp64" in which:
+        run_c4_fp64()

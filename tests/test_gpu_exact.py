@@ -108,6 +108,25 @@ def test_exact_gradient_matches_oracle(case, oracle_grad, cuda, ck_every, stream
     assert rel_err(m[0, 0].cpu().numpy(), gmt) < TOL_EXACT
 
 
+@pytest.mark.gpu
+def test_exact_fused_launches_match_two_pass_form(case, cuda):
+    """One gather launch per transposed half-step (default) against the per-cell pass +
+    gather form: same expressions, same results."""
+    from elastic_fm_vp_vs_rho_b200 import _lib
+    c = case
+    out = []
+    for fused in (1, 0):
+        b = _batch(c, 16)
+        b.set_option(_lib.EFM_OPT_EXACT_FUSED, fused)
+        mod = b.forward(checkpoints=True)
+        res, _ = b.residual_misfit(mod, cuda.as_tensor(c["obs"].reshape(-1)).cuda())
+        g, m = b.gradient(res, exact=True, mt=True)
+        out.append((g.cpu().numpy(), m.cpu().numpy()))
+        b.close()
+    assert rel_err(out[0][0], out[1][0]) < 1e-6
+    assert rel_err(out[0][1], out[1][1]) < 1e-6
+
+
 def _fd_directions(c):
     """Smooth seeded model directions (largest relative change 1) for each parameter."""
     from scipy.ndimage import gaussian_filter

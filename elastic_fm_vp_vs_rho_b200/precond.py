@@ -376,23 +376,8 @@ def _wolfe(prob, p, J, g, d, a0, tries=6, c1=1e-4, c2=0.9):
     return best
 
 
-def _secant_refine(prob, p, g, d, acc, lo=0.25, hi=4.0):
-    """One secant step on the directional derivative along d after an accepted trial
-    (a, J(a), g(a)): a' = a s0 / (s0 - s1) with s0 = g.d, s1 = g(a).d, clamped to
-    [lo a, hi a]; one more misfit + gradient evaluation, kept when its misfit is lower."""
-    a1, J1, g1 = acc
-    s0, s1 = _dot(g, d), _dot(g1, d)
-    if not (s0 < 0 and s1 != s0):
-        return acc
-    a2 = min(max(a1 * s0 / (s0 - s1), lo * a1), hi * a1)
-    if abs(a2 - a1) <= 0.1 * a1:
-        return acc
-    J2, g2 = prob.gradient(p + a2 * d)
-    return (a2, J2, g2) if math.isfinite(J2) and J2 < J1 else acc
-
-
 def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", log=None,
-           learned_iters=None, learned_tries=2, layers=7, refine=False):
+           learned_iters=None, learned_tries=2, layers=7):
     """Plain (net=None) or learned-direction inversion.  Returns a history of dicts
     (iteration, solves so far, misfit, model error, direction used).
 
@@ -402,8 +387,7 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", 
 
     learned_iters: use the network only in the first that many iterations (None: always);
     learned_tries: Wolfe trials a learned direction gets before the iteration falls back to
-    L-BFGS; refine: after an accepted learned step, one secant correction of its length
-    (2 more solves, kept when it lowers the misfit)."""
+    L-BFGS."""
     p = (prob.init / prob.scale).contiguous()
     lb = GpuLBFGS(p.shape, layers)
     prob.solves = 0
@@ -419,8 +403,6 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", 
             d = (out[..., :3].permute(3, 0, 1, 2) / GAIN).contiguous()
             if float(d.abs().max()) > 0:
                 acc = _wolfe(prob, p, J, g, d, 1.0, tries=learned_tries)
-                if acc is not None and refine:
-                    acc = _secant_refine(prob, p, g, d, acc)
                 used = "learned"
         if acc is None:
             d = lb.direction(g)
@@ -450,14 +432,22 @@ def invert(prob, iters, net=None, first_step=0.02, record=None, target="lbfgs", 
             log(f"it {it}: J {J:.4e} solves {prob.solves} ({used})")
     if record is not None:
         for f, pk, unit_step in kept:
-            if target == "error":
-                t = (prob.true / prob.scale - pk) * GAIN
-            elif target == "lbfgs":
-                t = (p - pk) * GAIN
+            if target == "raw":  # the ingredients of every target (experiment variants)
+                record.append((f, pk, unit_step, p, prob.true / prob.scale))
             else:
-                t = unit_step
-            record.append((f, t.permute(1, 2, 3, 0).contiguous()))
+                record.append((f, make_target(target, prob, pk, p, unit_step)))
     return hist
+
+
+def make_target(target, prob, pk, p_last, unit_step, true_norm=None):
+    """(ny, nz, nx, 3) training target of iterate pk of a plain run ending at p_last."""
+    if target == "error":
+        t = ((prob.true / prob.scale if true_norm is None else true_norm) - pk) * GAIN
+    elif target == "lbfgs":
+        t = (p_last - pk) * GAIN
+    else:
+        t = unit_step
+    return t.permute(1, 2, 3, 0).contiguous()
 
 
 def solves_to_reach(hist, target):
@@ -468,8 +458,7 @@ def solves_to_reach(hist, target):
 
 
 POLICIES = {"always": dict(learned_iters=None), "first2": dict(learned_iters=2),
-            "first4": dict(learned_iters=4),
-            "first2_refine": dict(learned_iters=2, refine=True)}
+            "first4": dict(learned_iters=4)}
 
 
 def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=12, epochs=40,
@@ -517,6 +506,54 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
                 summary=summary, tests=tests)
 
 
+def variant_experiment(variants, train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9),
+                       iters=10, spec=None, log=None, illumination=True, policy="first2"):
+    """Several networks trained on the SAME plain-L-BFGS runs (one data pass): each variant
+    is (target, epochs); on the unseen seeds every variant's learned run (one policy) is
+    compared with plain L-BFGS as in :func:`experiment`."""
+    import time
+    base = spec or ProblemSpec()
+    raw = []
+    t0 = time.time()
+    for s in train_seeds:
+        prob = InversionProblem(dataclasses.replace(base, seed=s), illumination)
+        invert(prob, iters, record=raw, target="raw")
+        prob.batch.close()
+    t_data = time.time() - t0
+    nets, info = {}, {}
+    for target, epochs in variants:
+        name = f"{target}_{epochs}"
+        samples = [(f, make_target(target, None, pk, pl, us, tn)) for f, pk, us, pl, tn in raw]
+        net = PreconditionerNet(seed=0, target=target)
+        losses = train(net, samples, epochs=epochs, log=log)
+        nets[name] = net
+        info[name] = dict(target=target, epochs=epochs, loss_first=losses[0], loss_last=losses[-1])
+        del samples
+    kw = POLICIES[policy]
+    tests = []
+    for ts in test_seeds:
+        prob = InversionProblem(dataclasses.replace(base, seed=ts), illumination)
+        plain = invert(prob, iters, log=log)
+        target_j = plain[-1]["misfit"]
+        row = dict(seed=ts, target_misfit=target_j, solves_plain=plain[-1]["solves"], variants={})
+        for name, net in nets.items():
+            h = invert(prob, iters, net=net, log=log, **kw)
+            row["variants"][name] = dict(solves=solves_to_reach(h, target_j),
+                                         final_misfit=h[-1]["misfit"],
+                                         fallbacks=sum(x["used"] == "fallback" for x in h))
+        prob.batch.close()
+        tests.append(row)
+    summary = {}
+    for name in nets:
+        sv = [t["variants"][name]["solves"] for t in tests]
+        plain_tot = sum(t["solves_plain"] for t in tests)
+        summary[name] = dict(info[name], solves=sv, solves_plain=[t["solves_plain"] for t in tests],
+                             total_ratio=(plain_tot / sum(sv)) if all(sv) else None)
+    return dict(spec=dataclasses.asdict(base), policy=policy, illumination=illumination,
+                train_seeds=list(train_seeds), test_seeds=list(test_seeds), iters=iters,
+                n_samples=len(raw), data_s=t_data, summary=summary, tests=tests)
+
+
 if __name__ == "__main__":
     import argparse
     import json
@@ -537,10 +574,26 @@ if __name__ == "__main__":
     ap.add_argument("--fq", type=float, default=12.0)
     ap.add_argument("--policies", default="first2,always", help="comma list of " + ",".join(POLICIES))
     ap.add_argument("--out", default=None)
+    ap.add_argument("--variants", default=None,
+                    help="target:epochs,... -- several networks trained on one data pass")
     a = ap.parse_args()
     gx, gy, gz = (int(v) for v in a.grid.split(","))
     spec = ProblemSpec(nx=gx, ny=gy, nz=gz, nt=a.nt, nshots=a.shots, nrec=a.receivers, dx=a.dx,
                        lenpml=a.lenpml, fq=a.fq)
+    if a.variants:
+        vs = [(t, int(e)) for t, e in (v.split(":") for v in a.variants.split(","))]
+        r = variant_experiment(vs, train_seeds=tuple(range(100, 100 + a.train)),
+                               test_seeds=tuple(int(v) for v in a.test_seeds.split(",")),
+                               iters=a.iters, spec=ProblemSpec(nx=gx, ny=gy, nz=gz, nt=a.nt,
+                                                               nshots=a.shots, nrec=a.receivers,
+                                                               dx=a.dx, lenpml=a.lenpml, fq=a.fq),
+                               log=print, illumination=not a.no_illumination,
+                               policy=a.policies.split(",")[0])
+        if a.out:
+            with open(a.out, "w") as f:
+                f.write(json.dumps(r, indent=1))
+        print(json.dumps(r["summary"]))
+        raise SystemExit(0)
     r = experiment(train_seeds=tuple(range(100, 100 + a.train)),
                    test_seeds=tuple(int(v) for v in a.test_seeds.split(",")),
                    iters=a.iters, epochs=a.epochs, spec=spec, target=a.target, log=print,

@@ -1381,6 +1381,11 @@ int efm_kernel_time(efm_ctx *ctx, int kind, int reps, int it, double *ms_per_lau
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    // the launches overwrote the wavefields: a gradient now needs a new forward first
+    for (Inst &I : ctx->inst) {
+        I.fwd_saved = false;
+        I.ck_saved = false;
+    }
     if (e != cudaSuccess) return fail(EFM_ERR_CUDA, std::string("efm_kernel_time: ") + cudaGetErrorString(e));
     *ms_per_launch = (double)ms / reps;
     return EFM_OK;

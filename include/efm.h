@@ -279,8 +279,8 @@ EFM_API int efm_kernel_stats(efm_ctx *ctx, int64_t *launches, double *ms, int re
  * forward stress / velocity after efm_forward, the two paired gradient launches and the
  * imaging after efm_gradient (plane-streaming kernels, paired launches); others give
  * EFM_ERR_STATE.  The launches overwrite the context's wavefields and add into the last
- * gradient buffer: run efm_forward again before the next efm_gradient.  No reference
- * counterpart (measurement only).
+ * gradient buffer: an efm_gradient now fails with EFM_ERR_STATE until efm_forward has run
+ * again.  No reference counterpart (measurement only).
  */
 EFM_API int efm_kernel_time(efm_ctx *ctx, int kind, int reps, int it, double *ms_per_launch,
                             void *stream);

@@ -158,7 +158,6 @@ struct efm_ctx {
     int opt_ck_every = 50;
     unsigned int opt_wait = 0;  // polls per tile wait (0: the kernels' default bound)
     int opt_exact_fused = 0;    // exact adjoint: 1 = one gather launch per transposed half-step
-    int opt_lane_map = 1;       // streaming forward/adjoint: x-CPML cells in the first warps
     // kernel kinds whose device tables (and tensor maps) are loaded now, for efm_kernel_time,
     // and the step count of those tables
     unsigned int timeable = 0;
@@ -620,7 +619,6 @@ int prepare_forward(efm_ctx *ctx, float *gathers, bool strips, bool recips, cuda
         d.nsteps = I.nt;
         d.err = ctx->d_err;
         d.wait_lim = ctx->opt_wait;
-        d.lane_map = ctx->opt_lane_map;
         for (int c = 0; c < 3; ++c) d.f.v[c] = d.f.vo[c] = I.va(c);
         for (int c = 0; c < 6; ++c) d.f.t[c] = I.tt(c);
         d.gather = gathers ? gathers + I.gather_off : nullptr;
@@ -1204,7 +1202,6 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
         a.nsteps = steps;
         a.err = ctx->d_err;
         a.wait_lim = ctx->opt_wait;
-        a.lane_map = ctx->opt_lane_map;
         for (int c = 0; c < 3; ++c) a.f.v[c] = a.f.vo[c] = I.bv(c);
         for (int c = 0; c < 6; ++c) a.f.t[c] = I.bt(c);
         a.res = res + I.gather_off;
@@ -1239,7 +1236,6 @@ int efm_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, int f
             r.nsteps = I.nt - 1;
             r.err = ctx->d_err;
             r.wait_lim = ctx->opt_wait;
-            r.lane_map = 0;
             r.k = -r.k;
             for (int c = 0; c < 3; ++c) {
                 r.f.v[c] = p == 0 ? I.va(c) : I.vb(c);
@@ -1420,7 +1416,6 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             ctx->opt_ring = value;
             break;
         case EFM_OPT_EXACT_FUSED: ctx->opt_exact_fused = value != 0; break;
-        case EFM_OPT_CPML_LANES: ctx->opt_lane_map = value != 0; break;
         case EFM_OPT_WAIT_LIMIT:
             if (value < 0) return fail(EFM_ERR_ARG, "wait limit must be >= 0 (0 = default)");
             ctx->opt_wait = (unsigned int)value;

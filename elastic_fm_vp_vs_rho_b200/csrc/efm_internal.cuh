@@ -74,7 +74,6 @@ struct EfmInst {
     const CUtensorMap *tmap;
     unsigned int *err;
     unsigned int wait_lim;  // polls per tile wait (0: the default bound; efm_mbar_wait)
-    int lane_map;           // streaming forward/adjoint: x-CPML cells packed into the first warps
     const float *rmu, *buoy;
     const uint8_t *rec_tile;
 };

@@ -137,47 +137,6 @@ __device__ __forceinline__ int stream_issuer(const Tile &T, int nx, int W) {
     return 0;
 }
 
-// Which cell of the tile this thread computes, as (lx, lr): cells (x0 + lx, z0 + lr + 4h).
-// Identity: lx = t % 64, lr = t / 64, and the issuing thread from stream_issuer.  With the
-// CPML lane map (forward and adjoint passes), in a tile that holds x-CPML columns the threads
-// are reassigned so that those columns' cells fill the first warps, in rank order, and every
-// other cell the warps after them: the memory-variable code then runs in ceil(n / 32) warps
-// (n = x-CPML cells of a plane's tile rows) instead of in every warp whose 32 x-columns touch
-// the slab, each with a third of its lanes busy.  Each cell is computed by the same
-// expressions either way, so the results do not change.  The issuing thread becomes lane 0 of
-// the first warp without x-CPML cells.  Reads only the tile's coordinates (before
-// efm_pdl_wait is fine).
-__device__ __forceinline__ void stream_lane_map(const Tile &T, int nx, int W, bool remap, int &lx,
-                                                int &lr, int &iss) {
-    __shared__ int s_cnt[EFM_STHREADS / 32];
-    __shared__ int s_perm[EFM_STHREADS];
-    const int t = threadIdx.x;
-    int p = t;
-    if (remap) {
-        const int x = T.x0 + t % EFM_STX;
-        const bool c = x < nx && (x < W || x >= nx - W);
-        const unsigned b = __ballot_sync(0xffffffffu, c);
-        const int lane = t & 31, warp = t >> 5;
-        if (lane == 0) s_cnt[warp] = __popc(b);
-        __syncthreads();
-        int off = 0, n = 0;
-#pragma unroll
-        for (int w = 0; w < EFM_STHREADS / 32; ++w) {
-            off += w < warp ? s_cnt[w] : 0;
-            n += s_cnt[w];
-        }
-        const int rank = off + __popc(b & ((1u << lane) - 1u));  // among the x-CPML positions
-        s_perm[c ? rank : n + (t - rank)] = t;
-        __syncthreads();
-        p = s_perm[t];
-        iss = min(32 * ((n + 31) / 32), EFM_STHREADS - 32);
-    } else {
-        iss = stream_issuer(T, nx, W);
-    }
-    lx = p % EFM_STX;
-    lr = p / EFM_STX;
-}
-
 // Block set-up shared by both kernels: barriers, prologue loads, source flag, receiver bits.
 template <int ROWS, int SR, int NH, int NC>
 __device__ __forceinline__ void stream_setup(const EfmInst &I, const Tile &T, Ring<ROWS, SR> &R,
@@ -486,11 +445,11 @@ __device__ __forceinline__ void stress_body(const EfmInst *__restrict__ insts, i
         T.ye = min(T.ye, ny - W);
         if (T.ys >= T.ye || T.z0 >= nz - W || T.x0 >= nx - W || T.x0 + EFM_STX <= W) return;
     }
-    int lx, lr, iss;
-    stream_lane_map(T, nx, W, PASS != EFM_REV && I.lane_map, lx, lr, iss);
+    const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
+    const int iss = stream_issuer(T, nx, W);
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const bool has_src = s_src != 0;
     unsigned int *const err = I.err;  // read once: the waits' clobbers would reload it
@@ -599,11 +558,11 @@ __device__ __forceinline__ void velocity_body(const EfmInst *__restrict__ insts,
         T.ye = min(T.ye, ny - W);
         if (T.ys >= T.ye || T.z0 >= nz - W || T.x0 >= nx - W || T.x0 + EFM_STX <= W) return;
     }
-    int lx, lr, iss;
-    stream_lane_map(T, nx, W, PASS != EFM_REV && I.lane_map, lx, lr, iss);
+    const int lx = threadIdx.x % EFM_STX, lr = threadIdx.x / EFM_STX;
     const int x = T.x0 + lx;
     const CUtensorMap *tm = I.tmap;
     Ring<ROWS, SR> R{smem, bars, NH * Ring<ROWS, SR>::HB + NC * Ring<ROWS, SR>::CB, NH, T.ys - 1};
+    const int iss = stream_issuer(T, nx, W);
     stream_setup<ROWS, SR, NH, NC>(I, T, R, tm, &s_src, &s_rec, iss);
     const unsigned long long recbits = s_rec;
     unsigned int *const err = I.err;  // read once: the waits' clobbers would reload it

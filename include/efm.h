@@ -237,11 +237,6 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
  * neighbours' terms.  Same expressions either way (no reference counterpart: the
  * reference has no exact adjoint). */
 #define EFM_OPT_EXACT_FUSED 10
-/* 1 (default): in the forward and adjoint plane-streaming kernels, the cells of a tile's
- * x-CPML columns are computed by the first warps of the block (packed by rank) instead of by
- * every warp whose x-columns touch the slab, so the memory-variable code runs in fewer
- * warps; 0: one thread per fixed (x, z) position.  Bit-identical either way. */
-#define EFM_OPT_CPML_LANES 11
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*

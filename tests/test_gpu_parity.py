@@ -342,52 +342,6 @@ def test_paired_gradient_launches_equal_sequential(golden_c1scale, cuda, rows, r
     assert np.array_equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("rows,ring", [(2, 4), (1, 4), (1, 6)])
-@pytest.mark.parametrize("grid", ["c1scale", "two_x_tiles"])
-def test_cpml_lane_map_is_bit_identical(golden_c1scale, cuda, rows, ring, grid):
-    """x-CPML cells packed into the first warps of a tile (EFM_OPT_CPML_LANES) give
-    bit-identical gathers and gradients: one 48-wide tile holding both x faces, and a
-    96-wide grid whose two tiles hold one face each."""
-    from elastic_fm_vp_vs_rho_b200 import ShotBatch, _lib, configs
-    d = golden_c1scale
-    if grid == "c1scale":
-        def make():
-            return _batch(d, d["lam0"], d["mu0"], d["rho0"], d["mt_obs"])
-        obs = cuda.as_tensor(d["obs0"].reshape(-1)).cuda()
-    else:
-        nx, ny, nz, W, dx = 96, 40, 36, 8, 10.0
-        vp, vs, rho = configs.layered_anomaly_model(ny, nz, nx, dx, seed=21, n_layers=3,
-                                                    n_anomalies=2, sigma_m=40.0, vpvs=1.8)
-        lam, mu = configs.lame_from_velocity(vp, vs, rho)
-        dt = configs.cfl_dt(dx, float(vp.max()))
-        nt = 160
-        cp = configs.cpml_profiles(12.0, dt, dx, W, float(vp.max()), nx, ny, nz)
-        rx, ry, rz = configs.surface_receivers(nx, ny, W, 6, 4)
-
-        def make():
-            b = ShotBatch()
-            b.add(nx=nx, ny=ny, nz=nz, lenpml=W, dx=dx, dt=dt, nt=nt, cpml=cp, lam=lam, mu=mu,
-                  rho=rho, wavelet=configs.ricker(12.0, dt, nt), src=[[48, 20, 18]],
-                  mt=[[0.4, -0.2, 0.6, 0.3, -0.5, 0.2]], rec=np.stack([rx, ry, rz], axis=1))
-            return b
-        obs = None
-    out = []
-    for lanes in (1, 0):
-        b = make()
-        b.set_option(_lib.EFM_OPT_TILE_ROWS, rows)
-        b.set_option(_lib.EFM_OPT_RING_DEPTH, ring)
-        b.set_option(_lib.EFM_OPT_CPML_LANES, lanes)
-        mod = b.forward(save_borders=True)
-        o = obs if obs is not None else mod * 0.5
-        res, _ = b.residual_misfit(mod, o)
-        g, m = b.gradient(res, model=True, mt=True)
-        b.status()
-        out.append((mod.cpu().numpy(), g.cpu().numpy(), m.cpu().numpy()))
-        b.close()
-    for a, r in zip(out[0], out[1]):
-        assert np.array_equal(a, r)
-
-
 def test_graph_replay_equals_step_launches(golden_c1scale, cuda):
     """Time loops captured as CUDA graphs and replayed (twice, the second call a pure replay)
     give bit-identical gathers, gradients and checkpointed states to step-by-step launches,

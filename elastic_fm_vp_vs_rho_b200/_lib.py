@@ -34,7 +34,9 @@ EFM_OPT_PAIR_LAUNCH = 6
 EFM_OPT_PDL = 7
 EFM_OPT_GRAPH = 8
 EFM_OPT_WAIT_LIMIT = 9
-EFM_OPT_EXACT_FUSED = 10
+EFM_OPT_EXACT_FORM = 10
+EFM_OPT_EXACT_FUSED = EFM_OPT_EXACT_FORM
+EFM_EXACT_TWO_PASS, EFM_EXACT_GATHER, EFM_EXACT_STREAM = 0, 1, 2
 EFM_NKERN = 11
 KERNEL_NAMES = ("fwd_stress", "fwd_velocity", "adj_stress", "adj_velocity", "rev_velocity",
                 "rev_stress", "residual_misfit", "model_reciprocals", "imaging",

@@ -34,6 +34,10 @@ extern "C" cudaError_t efm_launch_image(const EfmInst *insts, int ninst, int til
                                         cudaStream_t s);
 extern "C" cudaError_t efm_launch_exact(int kind, const EfmExact *t, int n, int tiles, int step,
                                         int slot, cudaStream_t s);
+extern "C" cudaError_t efm_launch_exact_stream(int kind, int rows, const EfmExact *t, int n,
+                                               int tiles, int step, int slot, cudaStream_t s);
+extern "C" int efm_exact_stream_tz(int rows);
+extern "C" int efm_exact_stream_blocks(int rows);
 extern "C" cudaError_t efm_launch_reciprocals(const float *mu, const float *rho, float *rmu,
                                               float *buoy, int64_t n, cudaStream_t s);
 
@@ -75,9 +79,11 @@ struct Inst {
     // exact adjoint: checkpoints of (v, tau, psi), a segment of per-step (v, tau), and the
     // adjoint memory variables (two sets, read / written alternately)
     float *ckpt = nullptr, *segbuf = nullptr, *apsi = nullptr;
-    float *exscr = nullptr;  // exact adjoint: 9 scratch volumes of the per-cell passes + 6 averages
+    float *exavg = nullptr;  // exact adjoint: the model's 6 harmonic-average volumes
+    float *exscr = nullptr;  // ... and the 9 scratch volumes of the per-cell + gather forms
     int ck_every = 0, nck = 0;
     bool ck_saved = false;
+    bool seg_saved = false;  // segbuf holds the last checkpoint segment of the last forward
     int64_t ncell = 0, strip_n = 0, psx_n = 0, psy_n = 0, psz_n = 0;
     int64_t gather_off = 0, grad_off = 0;
     int tiles_x = 0, tiles_z = 0, tiles_y = 0, tiles = 0, tile_begin = 0;
@@ -155,9 +161,11 @@ struct efm_ctx {
     int opt_pdl = 1;
     int rows = 2;  // cells per thread of the tables last built for the streaming kernels
     int ring = 4;  // ring depth of those tables' kernels
-    int opt_ck_every = 50;
+    int opt_ck_every = 0;       // 0: the longest interval whose workspace fits (checkpoint_interval)
+    int ck_auto = 0;            // that interval, chosen at the first allocation for the instance set
     unsigned int opt_wait = 0;  // polls per tile wait (0: the kernels' default bound)
-    int opt_exact_fused = 0;    // exact adjoint: 1 = one gather launch per transposed half-step
+    int opt_exact_form = 2;     // exact adjoint: 0 per-cell + gather launches, 1 one gather
+                                // launch, 2 one plane-streaming launch per transposed half-step
     // kernel kinds whose device tables (and tensor maps) are loaded now, for efm_kernel_time,
     // and the step count of those tables
     unsigned int timeable = 0;
@@ -361,7 +369,7 @@ int finish_table(EfmInst *t, int n) {
 
 // Planes per streaming block: the chunk that fills whole waves of blocks best, for tiles of
 // EFM_STX x tz cells and `per_sm` resident blocks per SM.
-int choose_ychunk(const efm_ctx *ctx, int tz, int per_sm) {
+int choose_ychunk(const efm_ctx *ctx, int tz, int per_sm, int tx = EFM_STX) {
     if (ctx->opt_ychunk > 0) return ctx->opt_ychunk;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
@@ -372,7 +380,7 @@ int choose_ychunk(const efm_ctx *ctx, int tz, int per_sm) {
     for (int yc = 4; yc <= EFM_MAX_YCHUNK; ++yc) {
         double blocks = 0;
         for (const auto &I : ctx->inst)
-            blocks += (double)((I.nx + EFM_STX - 1) / EFM_STX) * ((I.nz + tz - 1) / tz) *
+            blocks += (double)((I.nx + tx - 1) / tx) * ((I.nz + tz - 1) / tz) *
                       ((I.ny + yc - 1) / yc);
         const double waves = std::ceil(blocks / slots);
         const double fill = blocks / (waves * slots);
@@ -407,7 +415,8 @@ void free_inst(Inst &I) {
     cudaFree(I.segbuf);
     cudaFree(I.apsi);
     cudaFree(I.exscr);
-    I.ckpt = I.segbuf = I.apsi = I.exscr = nullptr;
+    cudaFree(I.exavg);
+    I.ckpt = I.segbuf = I.apsi = I.exscr = I.exavg = nullptr;
     I.ck_every = I.nck = 0;
     I.cpml = nullptr;
     I.rec_mask = nullptr;
@@ -572,23 +581,70 @@ int check_ready(efm_ctx *ctx) {
 
 size_t ckpt_floats(const Inst &I) { return 9 * (size_t)I.ncell + psi_floats(I); }
 
-// Workspace of the exact adjoint (checkpoint interval from the context option).
+// Exact-adjoint workspace of one instance at checkpoint interval K: nt/K - 1 checkpoints of
+// the fields and memory variables, a segment of K + 1 stored steps, the adjoint memory
+// variables (two parities) and the 6 harmonic-average volumes.
+size_t exact_bytes(const Inst &I, int K) {
+    K = std::max(1, std::min(K, I.nt));
+    const size_t nck = (size_t)std::max(1, (I.nt + K - 1) / K - 1);
+    return (nck * ckpt_floats(I) + (size_t)(K + 1) * 9 * I.ncell + 2 * psi_floats(I) +
+            6 * (size_t)I.ncell) * sizeof(float);
+}
+
+// Checkpoint interval: the option, or (option 0) the longest interval that splits the record
+// into equal segments and whose workspace for every instance fits in 60% of the free device
+// memory (the workspace this context holds counts as free).  Longer intervals replay fewer
+// steps (the exact gradient replays nt - K forward steps: all segments but the last, which
+// the forward keeps); below ~sqrt(nt) the checkpoints dominate, so the search stops there.
+int checkpoint_interval(efm_ctx *ctx) {
+    if (ctx->opt_ck_every > 0) return ctx->opt_ck_every;
+    if (ctx->ck_auto > 0) return ctx->ck_auto;
+    int nt = 1;
+    for (const Inst &I : ctx->inst) nt = std::max(nt, I.nt);
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        fr = 0;
+    }
+    size_t held = 0;
+    for (const Inst &I : ctx->inst)
+        if (I.ckpt != nullptr) held += exact_bytes(I, I.ck_every);
+    const double budget = 0.6 * (double)(fr + held);
+    const int kmin = std::max(1, (int)std::sqrt((double)nt));
+    int K = kmin;
+    for (int nseg = 1; nseg <= nt; ++nseg) {
+        const int k = (nt + nseg - 1) / nseg;
+        if (k < kmin) break;
+        double b = 0;
+        for (const Inst &I : ctx->inst) b += (double)exact_bytes(I, k);
+        if (b <= budget) {
+            K = k;
+            break;
+        }
+    }
+    return ctx->ck_auto = K;
+}
+
+// Workspace of the exact adjoint (checkpoint interval from checkpoint_interval).
 int ensure_exact(efm_ctx *ctx) {
+    const int Kc = checkpoint_interval(ctx);
     for (Inst &I : ctx->inst) {
-        const int K = std::max(1, std::min(ctx->opt_ck_every, I.nt));
+        const int K = std::max(1, std::min(Kc, I.nt));
         if (I.ckpt != nullptr && I.ck_every == K) continue;
         cudaFree(I.ckpt);
         cudaFree(I.segbuf);
         cudaFree(I.apsi);
         cudaFree(I.exscr);
-        I.ckpt = I.segbuf = I.apsi = I.exscr = nullptr;
+        cudaFree(I.exavg);
+        I.ckpt = I.segbuf = I.apsi = I.exscr = I.exavg = nullptr;
+        I.ck_saved = I.seg_saved = false;  // checkpoints of another interval are gone
         I.ck_every = K;
         I.nck = (I.nt + K - 1) / K;
         const size_t nck = (size_t)std::max(1, I.nck - 1);
         if (cudaMalloc(&I.ckpt, nck * ckpt_floats(I) * sizeof(float)) != cudaSuccess ||
             cudaMalloc(&I.segbuf, (size_t)(K + 1) * 9 * I.ncell * sizeof(float)) != cudaSuccess ||
             cudaMalloc(&I.apsi, 2 * psi_floats(I) * sizeof(float)) != cudaSuccess ||
-            cudaMalloc(&I.exscr, 15 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
+            cudaMalloc(&I.exavg, 6 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
             cudaGetLastError();
             return fail(EFM_ERR_NOMEM, "cannot allocate exact-adjoint checkpoints (interval " +
                                            std::to_string(K) + ")");
@@ -706,13 +762,25 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
         ctx->ex_cap = n;
     }
     std::vector<EfmExact> tab(2 * (size_t)n);
-    int tiles = 0;
+    int tiles = 0, st_tiles = 0;
+    const int xs_rows = ctx->opt_rows == 1 ? 1 : 2, xs_tz = efm_exact_stream_tz(xs_rows);
+    const int xs_yc = choose_ychunk(ctx, xs_tz, std::max(1, efm_exact_stream_blocks(xs_rows)), 32);
+    bool xs_fits = true;
+    for (const Inst &I : ctx->inst) xs_fits = xs_fits && I.ncell < ((int64_t)1 << 31) && psi_floats(I) < ((size_t)1 << 31);
     for (int i = 0; i < n; ++i) {
         Inst &I = ctx->inst[i];
         EFM_CK(cudaMemsetAsync(I.bv(0), 0, 9 * I.ncell * sizeof(float), s));
         EFM_CK(cudaMemsetAsync(I.apsi, 0, 2 * psi_floats(I) * sizeof(float), s));
-        // cells outside the update domain read zero from the scratch of the per-cell passes
-        EFM_CK(cudaMemsetAsync(I.exscr, 0, 15 * (size_t)I.ncell * sizeof(float), s));
+        // the per-cell + gather forms' scratch (allocated on first use); cells outside the
+        // update domain read zero from it
+        if (ctx->opt_exact_form != 2) {
+            if (I.exscr == nullptr &&
+                cudaMalloc(&I.exscr, 9 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(EFM_ERR_NOMEM, "cannot allocate the exact adjoint's scratch volumes");
+            }
+            EFM_CK(cudaMemsetAsync(I.exscr, 0, 9 * (size_t)I.ncell * sizeof(float), s));
+        }
         EFM_CK(cudaMemsetAsync(grad + I.grad_off, 0, 3 * I.ncell * sizeof(float), s));
         if (mt) EFM_CK(cudaMemsetAsync(mtg + (size_t)i * EFM_NSRC * 6, 0, EFM_NSRC * 6 * sizeof(double), s));
         EfmExact e;
@@ -726,6 +794,12 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
         e.tiles_y = (I.ny + EFM_TY - 1) / EFM_TY;
         e.tile_begin = tiles;
         tiles += e.tiles_x * e.tiles_z * e.tiles_y;
+        e.st_tx = (I.nx + 31) / 32;
+        e.st_tz = (I.nz + xs_tz - 1) / xs_tz;
+        e.ychunk = xs_yc;
+        e.st_ty = (I.ny + xs_yc - 1) / xs_yc;
+        e.st_begin = st_tiles;
+        st_tiles += e.st_tx * e.st_tz * e.st_ty;
         e.nt = I.nt;
         e.k = I.dt / I.dx;
         e.lam = I.lam;
@@ -743,7 +817,7 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
         e.g_mu = grad + I.grad_off + I.ncell;
         e.g_rho = grad + I.grad_off + 2 * I.ncell;
         e.scr = I.exscr;
-        e.avg = I.exscr + 9 * I.ncell;
+        e.avg = I.exavg;
         e.nsrc = I.nsrc;
         for (int q = 0; q < EFM_NSRC; ++q) {
             e.sx[q] = I.src[q][0];
@@ -777,9 +851,14 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
     const int K = ctx->inst[0].ck_every;
     const int nseg = (nt + K - 1) / K;
     int parity = 0;
+    bool kept = true;
+    for (const Inst &I : ctx->inst) kept = kept && I.seg_saved && I.nck == nseg;
     for (int k = nseg - 1; k >= 0; --k) {
         const int first = k * K, last = std::min(nt, first + K) - 1;
+        for (Inst &I : ctx->inst) I.seg_saved = false;  // segbuf is rewritten below
+        const bool replay = !(kept && k == nseg - 1);
         for (Inst &I : ctx->inst) {
+            if (!replay) break;
             if (k == 0) {
                 EFM_CK(cudaMemsetAsync(I.fields, 0, 9 * I.ncell * sizeof(float), s));
                 if ((rc = zero_psi(I, s))) return rc;
@@ -793,7 +872,7 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
             EFM_CK(cudaMemcpyAsync(I.segbuf, I.fields, 9 * I.ncell * sizeof(float),
                                    cudaMemcpyDeviceToDevice, s));
         }
-        for (int it = first; it <= last; ++it) {
+        for (int it = first; it <= last && replay; ++it) {
             if ((rc = forward_step(ctx, st, it, s))) return rc;
             for (Inst &I : ctx->inst)
                 EFM_CK(cudaMemcpyAsync(I.segbuf + (size_t)(it - first + 1) * 9 * I.ncell, I.fields,
@@ -806,13 +885,17 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
                      return efm_launch_exact(0, t, n, 0, it, slot, s);
                  })))
                 return rc;
-            const int kv = ctx->opt_exact_fused ? 4 : 1, ks = ctx->opt_exact_fused ? 5 : 2;
+            // the streaming form indexes cells with 32-bit offsets
+            const int form = (ctx->opt_exact_form == 2 && !xs_fits) ? 0 : ctx->opt_exact_form;
+            const int kv = form == 1 ? 4 : 1, ks = form == 1 ? 5 : 2;
             if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
-                     return efm_launch_exact(kv, t, n, tiles, it, slot, s);
+                     return form == 2 ? efm_launch_exact_stream(0, xs_rows, t, n, st_tiles, it, slot, s)
+                                      : efm_launch_exact(kv, t, n, tiles, it, slot, s);
                  })))
                 return rc;
             if ((rc = timed_launch(ctx, EFM_K_ADJ_STRESS, s, [&] {
-                     return efm_launch_exact(ks, t, n, tiles, it, slot, s);
+                     return form == 2 ? efm_launch_exact_stream(1, xs_rows, t, n, st_tiles, it, slot, s)
+                                      : efm_launch_exact(ks, t, n, tiles, it, slot, s);
                  })))
                 return rc;
             parity ^= 1;
@@ -905,6 +988,7 @@ int efm_clear(efm_ctx *ctx) {
     if (ctx == nullptr) return fail(EFM_ERR_ARG, "null context");
     for (Inst &I : ctx->inst) free_inst(I);
     ctx->inst.clear();
+    ctx->ck_auto = 0;
     ctx->layout_ready = false;
     ctx->timeable = 0;
     drop_loops(ctx);
@@ -1042,6 +1126,7 @@ int efm_add_instance(efm_ctx *ctx, const efm_instance_desc *d, int *id) {
         if ((e = cudaMemcpy(I.rec_tile, rt.data(), rt.size(), cudaMemcpyHostToDevice))) return bad(e);
     }
     ctx->inst.push_back(std::move(I));
+    ctx->ck_auto = 0;  // the automatic checkpoint interval is chosen for the new instance set
     ctx->layout_ready = false;
     if (id) *id = (int)ctx->inst.size() - 1;
     return EFM_OK;
@@ -1121,13 +1206,24 @@ int efm_forward_illumination(efm_ctx *ctx, float *gathers, int save, float *illu
         for (const Inst &I : ctx->inst)
             key.insert(key.end(), {I.ck_every, I.nt, (int64_t)(uintptr_t)I.ckpt,
                                    (int64_t)(uintptr_t)I.fields, (int64_t)(uintptr_t)I.psi,
-                                   I.ncell, (int64_t)psi_floats(I)});
+                                   (int64_t)(uintptr_t)I.segbuf, I.ncell, (int64_t)psi_floats(I)});
+    // The exact gradient replays the segments last to first from their checkpoints; the last
+    // one is kept here as it is computed (slot 0: the state before its first step, slot s: after
+    // its s-th step), so the gradient recomputes one segment fewer.
+    auto last_first = [](const Inst &I) { return (I.nck - 1) * I.ck_every; };
+    auto keep = [&](Inst &I, int slot, cudaStream_t ls) {
+        return cudaMemcpyAsync(I.segbuf + (size_t)slot * 9 * I.ncell, I.fields,
+                               9 * I.ncell * sizeof(float), cudaMemcpyDeviceToDevice, ls);
+    };
     rc = run_loop(ctx, 0, key, s, [&](cudaStream_t ls) {
         int r;
+        if (ckpts)
+            for (Inst &I : ctx->inst)
+                if (last_first(I) == 0) EFM_CK(keep(I, 0, ls));
         for (int it = 0; it < maxnt; ++it) {
             if ((r = forward_step(ctx, st, it, ls, illum != nullptr))) return r;
             if (ckpts)
-                for (Inst &I : ctx->inst)
+                for (Inst &I : ctx->inst) {
                     if ((it + 1) % I.ck_every == 0 && it + 1 < I.nt) {
                         // checkpoint k = (it+1)/K holds the state after step it (k >= 1; 0 = zeros)
                         float *dst = I.ckpt + (size_t)((it + 1) / I.ck_every - 1) * ckpt_floats(I);
@@ -1136,6 +1232,8 @@ int efm_forward_illumination(efm_ctx *ctx, float *gathers, int save, float *illu
                         EFM_CK(cudaMemcpyAsync(dst + 9 * I.ncell, I.psi, psi_floats(I) * sizeof(float),
                                                cudaMemcpyDeviceToDevice, ls));
                     }
+                    if (it < I.nt && it + 1 >= last_first(I)) EFM_CK(keep(I, it + 1 - last_first(I), ls));
+                }
         }
         return (int)EFM_OK;
     });
@@ -1143,6 +1241,7 @@ int efm_forward_illumination(efm_ctx *ctx, float *gathers, int save, float *illu
     for (Inst &I : ctx->inst) {
         I.fwd_saved = strips;
         I.ck_saved = ckpts;
+        I.seg_saved = ckpts;
     }
     if (st && illum == nullptr) {
         ctx->timeable = (1u << EFM_K_FWD_STRESS) | (1u << EFM_K_FWD_VELOCITY);
@@ -1401,8 +1500,10 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             ctx->opt_ychunk = value;
             break;
         case EFM_OPT_CHECKPOINT_EVERY:
-            if (value < 1 || value > 100000) return fail(EFM_ERR_ARG, "checkpoint interval must be >= 1");
+            if (value < 0 || value > 100000)
+                return fail(EFM_ERR_ARG, "checkpoint interval must be >= 1 (0: automatic)");
             ctx->opt_ck_every = value;
+            ctx->ck_auto = 0;
             break;
         case EFM_OPT_TILE_ROWS:
             if (value < 0 || value > 2) return fail(EFM_ERR_ARG, "tile rows must be 0, 1 or 2");
@@ -1415,7 +1516,10 @@ int efm_set_option(efm_ctx *ctx, int option, int value) {
             if (value != 0 && value != 4 && value != 6) return fail(EFM_ERR_ARG, "ring depth must be 0, 4 or 6");
             ctx->opt_ring = value;
             break;
-        case EFM_OPT_EXACT_FUSED: ctx->opt_exact_fused = value != 0; break;
+        case EFM_OPT_EXACT_FORM:
+            if (value < 0 || value > 2) return fail(EFM_ERR_ARG, "EFM_OPT_EXACT_FORM must be 0, 1 or 2");
+            ctx->opt_exact_form = value;
+            break;
         case EFM_OPT_WAIT_LIMIT:
             if (value < 0) return fail(EFM_ERR_ARG, "wait limit must be >= 0 (0 = default)");
             ctx->opt_wait = (unsigned int)value;

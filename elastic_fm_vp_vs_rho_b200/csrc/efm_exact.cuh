@@ -1,4 +1,5 @@
-// Table entry of the exact-adjoint kernels (efm_exact.cu), one per instance.
+// Table entry of the exact-adjoint kernels (efm_exact.cu, efm_exact_stream.cu), one per
+// instance.
 #pragma once
 #include <stdint.h>
 
@@ -6,11 +7,12 @@
 
 struct EfmExact {
     int nx, ny, nz, W;
-    int tiles_x, tiles_z, tiles_y, tile_begin;
+    int tiles_x, tiles_z, tiles_y, tile_begin;   // one-thread-per-cell kernels
+    int st_tx, st_tz, st_ty, st_begin, ychunk;   // plane-streaming kernels (efm_exact_stream.cu)
     int nt;
     float k;
     const float *lam, *mu, *rho, *cpml;
-    float *bv[3], *bt[6];
+    float *bv[3], *bt[6];   // nine consecutive volumes (the streaming kernels use stride N)
     const float *pin;   // adjoint memory variables, read (x, y, z slab families, 6 vars each)
     float *pout;        // ... written
     int64_t psx_n, psy_n, psz_n;

@@ -1,5 +1,6 @@
 """Device time of one gradient evaluation: the reference-mode imaging gradient against the
-exact discrete adjoint (fused and two-pass transposed half-steps).
+exact discrete adjoint: plane-streaming transposed half-steps with the automatic checkpoint
+interval and with 50-step checkpoints, and the two-pass and single-gather forms (50-step).
 
     python -m elastic_fm_vp_vs_rho_b200.gradbench [--grid 128,128,96] [--nt 300] [--reps 3]
 
@@ -51,9 +52,13 @@ def main(argv=None):
         eng.gradient(res, model=True, mt=True, exact=exact)
 
     out = {"workload": w.name, "grid": [w.nx, w.ny, w.nz], "nt": w.nt}
-    for label, exact, fused in (("imaging", False, 1), ("exact_fused", True, 1),
-                                ("exact_two_pass", True, 0)):
-        eng.set_option(_lib.EFM_OPT_EXACT_FUSED, fused)
+    for label, exact, form, K in (("imaging", False, 2, 0),
+                                  ("exact_stream", True, _lib.EFM_EXACT_STREAM, 0),
+                                  ("exact_stream_k50", True, _lib.EFM_EXACT_STREAM, 50),
+                                  ("exact_two_pass_k50", True, _lib.EFM_EXACT_TWO_PASS, 50),
+                                  ("exact_gather_k50", True, _lib.EFM_EXACT_GATHER, 50)):
+        eng.set_option(_lib.EFM_OPT_EXACT_FORM, form)
+        eng.set_option(_lib.EFM_OPT_CHECKPOINT_EVERY, K)
         run(exact)
         torch.cuda.synchronize()
         times = []
@@ -76,7 +81,7 @@ def main(argv=None):
                       "per_kernel_ms": {k: round(ms[i], 2) for i, k in enumerate(_lib.KERNEL_NAMES)
                                         if n[i]}}
     eng.status()
-    out["exact_over_imaging"] = out["exact_fused"]["ms"] / out["imaging"]["ms"]
+    out["exact_over_imaging"] = out["exact_stream"]["ms"] / out["imaging"]["ms"]
     print(json.dumps(out))
     eng.close()
 

@@ -42,7 +42,9 @@ def instance_bytes(nx, ny, nz, lenpml, nt, nrec=0, gradient="imaging", ck_every=
     elif gradient == "exact":
         K = max(1, min(ck_every, nt))
         nck = (nt + K - 1) // K
-        b += nck * (9 * ncell + psi) * 4 + (K + 1) * 9 * ncell * 4 + 2 * psi * 4 + 15 * ncell * 4
+        # checkpoints, the stored segment, adjoint memory variables, harmonic averages (the
+        # per-cell + gather forms of EFM_OPT_EXACT_FORM add 9 scratch volumes)
+        b += nck * (9 * ncell + psi) * 4 + (K + 1) * 9 * ncell * 4 + 2 * psi * 4 + 6 * ncell * 4
     else:
         raise ValueError(f"unknown gradient kind {gradient!r}")
     return b

@@ -203,8 +203,12 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
 /* Planes per block of the plane-streaming kernels; 0 (default) picks the chunk that fills
  * whole waves of blocks best. */
 #define EFM_OPT_YCHUNK 2
-/* Steps between full-state checkpoints of EFM_SAVE_CHECKPOINTS (default 50); memory per
- * instance ~ (nt/K) checkpoints + (K+1) stored steps of the 9 fields. */
+/* Steps K between full-state checkpoints of EFM_SAVE_CHECKPOINTS; memory per instance ~
+ * (nt/K - 1) checkpoints + (K+1) stored steps of the 9 fields.  The exact gradient replays
+ * nt - K forward steps (the forward keeps the last segment).  0 (default): the longest K
+ * that splits nt into equal segments and whose workspace for all instances fits in 60% of
+ * the free device memory when it is first allocated (K = nt, no replay, when it fits; at
+ * least ~sqrt(nt), the smallest-memory interval). */
 #define EFM_OPT_CHECKPOINT_EVERY 3
 /* Cells per thread of the plane-streaming stress/velocity kernels: 2 (64 x 8 tiles, two
  * blocks per SM) or 1 (64 x 4 tiles, three blocks per SM); 0 (default) = 2. */
@@ -232,11 +236,17 @@ EFM_API int efm_residual_misfit_noalloc(const float *mod_dev, const float *obs_d
  * limit is unaffected.  Small values exist for failure-detection tests (no reference
  * counterpart; the reference's kernels have no waits). */
 #define EFM_OPT_WAIT_LIMIT 9
-/* EFM_GRAD_EXACT: 0 (default) runs each transposed half-step as a per-cell pass into
- * scratch volumes + a gather launch; 1 as one gather launch that recomputes its
- * neighbours' terms.  Same expressions either way (no reference counterpart: the
- * reference has no exact adjoint). */
-#define EFM_OPT_EXACT_FUSED 10
+/* EFM_GRAD_EXACT: how each transposed half-step runs.  2 (default): one plane-streaming
+ * launch (each block marches a 32 x 16 column of cells along y, 32 x 8 with
+ * EFM_OPT_TILE_ROWS = 1; y-chunk from EFM_OPT_YCHUNK or chosen for full waves); 0: a
+ * per-cell pass into scratch volumes + a gather launch; 1: one gather launch that recomputes
+ * its neighbours' terms.  Same expressions in every form; the streaming form adds a few
+ * terms in another order (no reference counterpart: the reference has no exact adjoint). */
+#define EFM_OPT_EXACT_FORM 10
+#define EFM_OPT_EXACT_FUSED EFM_OPT_EXACT_FORM  /* earlier name */
+#define EFM_EXACT_TWO_PASS 0
+#define EFM_EXACT_GATHER 1
+#define EFM_EXACT_STREAM 2
 EFM_API int efm_set_option(efm_ctx *ctx, int option, int value);
 
 /*

@@ -91,7 +91,7 @@ def _batch(c, ck_every, stream=1):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ck_every,stream", [(16, 1), (60, 1), (7, 0)])
+@pytest.mark.parametrize("ck_every,stream", [(16, 1), (60, 1), (7, 0), (0, 1)])
 def test_exact_gradient_matches_oracle(case, oracle_grad, cuda, ck_every, stream):
     c = case
     J, gl, gm, gr, gmt = oracle_grad
@@ -108,16 +108,66 @@ def test_exact_gradient_matches_oracle(case, oracle_grad, cuda, ck_every, stream
     assert rel_err(m[0, 0].cpu().numpy(), gmt) < TOL_EXACT
 
 
+def _form_batch(ck_every=10):
+    """Two instances of different grids in one batch: 70 x 30 x 37 (three 32-wide x tiles,
+    the last partial; z tiles of 16 or 8 rows, the last partial) with three sources, one on
+    a tile corner and one next to it, and 40 x 26 x 21 with one source."""
+    from elastic_fm_vp_vs_rho_b200 import ShotBatch, _lib
+    b = ShotBatch()
+    for (nx, ny, nz, W, seed, src) in ((70, 30, 37, 6, 9, [(32, 15, 16), (31, 14, 15), (63, 16, 31)]),
+                                       (40, 26, 21, 5, 4, [(20, 12, 9)])):
+        dx = 10.0
+        vp, vs, rho = configs.layered_anomaly_model(ny, nz, nx, dx, seed=seed, n_layers=3,
+                                                    n_anomalies=2, sigma_m=40, vpvs=1.8)
+        lam, mu = configs.lame_from_velocity(vp, vs, rho)
+        dt = configs.cfl_dt(dx, float(vp.max()))
+        nt = 40
+        rng = np.random.default_rng(seed)
+        mt = rng.standard_normal((len(src), 6))
+        rx, ry, rz = configs.surface_receivers(nx, ny, W, 5, 4)
+        b.add(nx=nx, ny=ny, nz=nz, lenpml=W, dx=dx, dt=dt, nt=nt,
+              cpml=configs.cpml_profiles(20.0, dt, dx, W, float(vp.max()), nx, ny, nz),
+              lam=lam, mu=mu, rho=rho, wavelet=configs.ricker(20.0, dt, nt), src=src, mt=mt,
+              rec=np.stack((rx, ry, rz), axis=1))
+    b.set_option(_lib.EFM_OPT_CHECKPOINT_EVERY, ck_every)
+    return b
+
+
+@pytest.mark.gpu
+def test_exact_stream_form_matches_two_pass_form(cuda):
+    """The plane-streaming transposes (default form) against the per-cell pass + gather form
+    on a batch of two grids, for both tile heights and several y-chunks (chunks of 5 and 7
+    planes put chunk seams inside the CPML slabs and next to the sources; 64 gives one
+    chunk)."""
+    from elastic_fm_vp_vs_rho_b200 import _lib
+    out = {}
+    for form, rows, yc in ((0, 2, 0), (2, 2, 0), (2, 1, 0), (2, 2, 5), (2, 2, 64), (2, 1, 7)):
+        b = _form_batch()
+        b.set_option(_lib.EFM_OPT_EXACT_FORM, form)
+        b.set_option(_lib.EFM_OPT_TILE_ROWS, rows)
+        b.set_option(_lib.EFM_OPT_YCHUNK, yc)
+        mod = b.forward(checkpoints=True)
+        g, m = b.gradient(mod, exact=True, mt=True)
+        b.status()
+        out[(form, rows, yc)] = (g.cpu().numpy(), m.cpu().numpy())
+        b.close()
+    g0, m0 = out.pop((0, 2, 0))
+    assert np.abs(g0).max() > 0 and np.abs(m0).max() > 0
+    for key, (g, m) in out.items():
+        assert rel_err(g, g0) < 1e-6, key
+        assert rel_err(m, m0) < 1e-6, key
+
+
 @pytest.mark.gpu
 def test_exact_fused_launches_match_two_pass_form(case, cuda):
-    """One gather launch per transposed half-step (default) against the per-cell pass +
-    gather form: same expressions, same results."""
+    """One gather launch per transposed half-step against the per-cell pass + gather form:
+    same expressions, same results."""
     from elastic_fm_vp_vs_rho_b200 import _lib
     c = case
     out = []
     for fused in (1, 0):
         b = _batch(c, 16)
-        b.set_option(_lib.EFM_OPT_EXACT_FUSED, fused)
+        b.set_option(_lib.EFM_OPT_EXACT_FORM, fused)
         mod = b.forward(checkpoints=True)
         res, _ = b.residual_misfit(mod, cuda.as_tensor(c["obs"].reshape(-1)).cuda())
         g, m = b.gradient(res, exact=True, mt=True)

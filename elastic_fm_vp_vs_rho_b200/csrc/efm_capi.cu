@@ -766,7 +766,8 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
     const int xs_rows = ctx->opt_rows == 1 ? 1 : 2, xs_tz = efm_exact_stream_tz(xs_rows);
     const int xs_yc = choose_ychunk(ctx, xs_tz, std::max(1, efm_exact_stream_blocks(xs_rows)), 32);
     bool xs_fits = true;
-    for (const Inst &I : ctx->inst) xs_fits = xs_fits && I.ncell < ((int64_t)1 << 31) && psi_floats(I) < ((size_t)1 << 31);
+    for (const Inst &I : ctx->inst)
+        xs_fits = xs_fits && 9 * I.ncell < ((int64_t)1 << 31) && psi_floats(I) < ((size_t)1 << 31);
     for (int i = 0; i < n; ++i) {
         Inst &I = ctx->inst[i];
         EFM_CK(cudaMemsetAsync(I.bv(0), 0, 9 * I.ncell * sizeof(float), s));
@@ -885,7 +886,7 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
                      return efm_launch_exact(0, t, n, 0, it, slot, s);
                  })))
                 return rc;
-            // the streaming form indexes cells with 32-bit offsets
+            // the streaming form indexes cells with 32-bit offsets (instances below ~238 M cells)
             const int form = (ctx->opt_exact_form == 2 && !xs_fits) ? 0 : ctx->opt_exact_form;
             const int kv = form == 1 ? 4 : 1, ks = form == 1 ? 5 : 2;
             if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {

@@ -274,7 +274,7 @@ enum { VT_G0, VT_G1, VT_G2, VT_Q0, VT_G6, VT_G7, VT_G8, VT_Q2, VT_NF };
 // (stride N cells): B_i (harmonic buoyancies), vbar_i, v_i^n, v_i^{n-1}.
 struct VtVol {
     const float *B, *v, *n, *m;
-    int64_t N;
+    int N;  // 9 N < 2^31 (host check): every offset below is a 32-bit integer
 };
 
 struct VtRaw {
@@ -338,14 +338,14 @@ __device__ __forceinline__ void vt_halo_load(const VtVol &V, const XsPsiPtr &Q, 
     const float *ps = xf ? Q.x : Q.z;
     const int pst = xf ? Q.sx : Q.sz, pi = xf ? xs_ix(R, k) : xs_iz(R, k);
     if (kind == XS_ZLO || kind == XS_XLO) {
-        const int64_t o = (kind == XS_XLO ? 0 : 2) * V.N + c;
+        const int o = (kind == XS_XLO ? 0 : 2) * V.N + c;
         d[0] = __ldg(V.B + o);
         d[1] = __ldg(V.v + o);
         d[2] = __ldg(V.n + o);
         d[3] = __ldg(V.m + o);
         if (sl) d[4] = ps[pi];
     } else {
-        const int64_t o = (kind == XS_XHI ? 1 : 0) * V.N + c;
+        const int o = (kind == XS_XHI ? 1 : 0) * V.N + c;
         d[0] = __ldg(V.B + o);
         d[1] = __ldg(V.v + o);
         d[2] = __ldg(V.B + o + V.N);
@@ -398,7 +398,7 @@ efm_exact_vt_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
     const XsC C = xs_consts(I);
     const XsTile T = xs_tile<ROWS>(I);
     VtVol V;
-    V.N = C.N;
+    V.N = (int)C.N;
     V.B = I.avg + 3 * C.N;
     V.v = I.bv[0];
     V.n = I.seg + (int64_t)slot * I.slot_stride;
@@ -407,6 +407,7 @@ efm_exact_vt_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
     const float kdt = C.k;
     float *const bt = I.bt[0];  // six consecutive volumes
     float *const grho = I.g_rho;
+    const int N = (int)C.N;
     const int lx = threadIdx.x & 31, lr = threadIdx.x >> 5;
     int hx, hz;
     const int duty = xs_duty<ROWS>(T, false, hx, hz);
@@ -455,7 +456,7 @@ efm_exact_vt_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
             const int c = base + col[h].off;
             const bool in = iny && (col[h].flags & XS_INXZ), gd = gdy && (col[h].flags & XS_GDXZ);
 #pragma unroll
-            for (int q = 0; q < 6; ++q) ob[h][q] = in ? bt[q * C.N + c] : 0.f;
+            for (int q = 0; q < 6; ++q) ob[h][q] = in ? bt[q * N + c] : 0.f;
             orh[h] = gd ? grho[c] : 0.f;
         }
         plane(j + 1, bn, j + 1 < T.ye, nxt);
@@ -470,13 +471,12 @@ efm_exact_vt_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
                 // taubar += D_T^T gbar
                 const float *G0 = S + VT_G0 * PL, *G1 = S + VT_G1 * PL, *G2 = S + VT_G2 * PL;
                 const float *G6 = S + VT_G6 * PL, *G7 = S + VT_G7 * PL, *G8 = S + VT_G8 * PL;
-                float *o = bt + c;
-                o[0] = ob[h][0] + (G0[si - 1] - G0[si]);
-                o[C.N] = ob[h][1] + (prv[h].g3 - cur[h].g3);
-                o[2 * C.N] = ob[h][2] + (G6[si - XS_PW] - G6[si]);
-                o[3 * C.N] = ob[h][3] + (cur[h].g4 - nxt[h].g4 + G1[si] - G1[si + 1]);
-                o[4 * C.N] = ob[h][4] + (G7[si] - G7[si + XS_PW] + G2[si] - G2[si + 1]);
-                o[5 * C.N] = ob[h][5] + (G8[si] - G8[si + XS_PW] + cur[h].g5 - nxt[h].g5);
+                bt[c] = ob[h][0] + (G0[si - 1] - G0[si]);
+                bt[N + c] = ob[h][1] + (prv[h].g3 - cur[h].g3);
+                bt[2 * N + c] = ob[h][2] + (G6[si - XS_PW] - G6[si]);
+                bt[3 * N + c] = ob[h][3] + (cur[h].g4 - nxt[h].g4 + G1[si] - G1[si + 1]);
+                bt[4 * N + c] = ob[h][4] + (G7[si] - G7[si + XS_PW] + G2[si] - G2[si + 1]);
+                bt[5 * N + c] = ob[h][5] + (G8[si] - G8[si + XS_PW] + cur[h].g5 - nxt[h].g5);
             }
             // rho gradient: -1/2 sum_i (q_i(p) + q_i(p - e_i))
             const float *Q0 = S + VT_Q0 * PL, *Q2 = S + VT_Q2 * PL;
@@ -513,7 +513,7 @@ enum { ST_D0, ST_D1, ST_D2, ST_D6, ST_D7, ST_D8, ST_UXY, ST_UYZ, ST_TXZ, ST_NF }
 // (stride N cells), taubar (6), the harmonic mu_xy, mu_xz, mu_yz (3), tau^n and tau^{n-1} (6).
 struct StVol {
     const float *lam, *mu, *b, *m, *n, *o;
-    int64_t N;
+    int N;  // 9 N < 2^31 (host check)
 };
 
 struct StRaw {
@@ -624,7 +624,7 @@ __device__ __forceinline__ void st_halo_load(const StVol &V, const XsPsiPtr &Q, 
     const int pst = xf ? Q.sx : Q.sz, pi = xf ? xs_ix(R, k) : xs_iz(R, k);
     if (kind == XS_ZLO || kind == XS_XLO || kind == XS_CORNER) {
         // shear components (3 + i0, 3 + i1): xz, yz (z-lo); xy, xz (x-lo); xz (corner)
-        const int64_t o0 = (kind == XS_XLO ? 0 : 1) * V.N + c, o1 = o0 + V.N;
+        const int o0 = (kind == XS_XLO ? 0 : 1) * V.N + c, o1 = o0 + V.N;
         d[0] = __ldg(V.b + 3 * V.N + o0);
         d[1] = __ldg(V.m + o0);
         d[2] = __ldg(V.n + 3 * V.N + o0) - __ldg(V.o + 3 * V.N + o0);
@@ -724,7 +724,7 @@ efm_exact_st_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
     const XsC C = xs_consts(I);
     const XsTile T = xs_tile<ROWS>(I);
     StVol V;
-    V.N = C.N;
+    V.N = (int)C.N;
     V.lam = I.lam;
     V.mu = I.mu;
     V.b = I.bt[0];
@@ -735,6 +735,7 @@ efm_exact_st_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
     const StSrc SR{&I, step};
     const float kdt = C.k;
     float *const bv = I.bv[0];  // three consecutive volumes
+    const int N = (int)C.N;
     float *const glam = I.g_lam, *const gmu = I.g_mu;
     const int lx = threadIdx.x & 31, lr = threadIdx.x >> 5;
     const int x = T.x0 + lx;
@@ -793,7 +794,7 @@ efm_exact_st_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
             const int c = base + col[h].off;
             const bool in = iny && (col[h].flags & XS_INXZ), gd = gdy && (col[h].flags & XS_GDXZ);
 #pragma unroll
-            for (int q = 0; q < 3; ++q) ov[h][q] = in ? bv[q * C.N + c] : 0.f;
+            for (int q = 0; q < 3; ++q) ov[h][q] = in ? bv[q * N + c] : 0.f;
             ol[h] = in ? glam[c] : 0.f;
             om[h] = gd ? gmu[c] : 0.f;
         }
@@ -809,10 +810,9 @@ efm_exact_st_stream(const EfmExact *__restrict__ t, int n, int step, int slot) {
                 // vbar += D_V^T dbar
                 const float *D0 = S + ST_D0 * PL, *D1 = S + ST_D1 * PL, *D2 = S + ST_D2 * PL;
                 const float *D6 = S + ST_D6 * PL, *D7 = S + ST_D7 * PL, *D8 = S + ST_D8 * PL;
-                float *o = bv + c;
-                o[0] = ov[h][0] + (D0[si] - D0[si + 1] + D7[si - XS_PW] - D7[si] + prv[h].d4 - cur[h].d4);
-                o[C.N] = ov[h][1] + (cur[h].d3 - nxt[h].d3 + D1[si - 1] - D1[si] + D8[si - XS_PW] - D8[si]);
-                o[2 * C.N] = ov[h][2] + (D6[si] - D6[si + XS_PW] + D2[si - 1] - D2[si] + prv[h].d5 - cur[h].d5);
+                bv[c] = ov[h][0] + (D0[si] - D0[si + 1] + D7[si - XS_PW] - D7[si] + prv[h].d4 - cur[h].d4);
+                bv[N + c] = ov[h][1] + (cur[h].d3 - nxt[h].d3 + D1[si - 1] - D1[si] + D8[si - XS_PW] - D8[si]);
+                bv[2 * N + c] = ov[h][2] + (D6[si] - D6[si + XS_PW] + D2[si - 1] - D2[si] + prv[h].d5 - cur[h].d5);
                 glam[c] = ol[h] + cur[h].dl;
             }
             // shear mu terms of the pairs xy, xz, yz

@@ -62,6 +62,12 @@ def test_argument_errors_return_status():
         assert L.efm_set_option(ctx, _lib.EFM_OPT_WAIT_LIMIT, -1) == _lib.EFM_ERR_ARG
         assert L.efm_set_option(ctx, _lib.EFM_OPT_WAIT_LIMIT, 4) == _lib.EFM_OK
         assert L.efm_set_option(ctx, _lib.EFM_OPT_WAIT_LIMIT, 0) == _lib.EFM_OK
+        assert L.efm_set_option(ctx, _lib.EFM_OPT_EXACT_FORM, 3) == _lib.EFM_ERR_ARG
+        for form in (_lib.EFM_EXACT_TWO_PASS, _lib.EFM_EXACT_GATHER, _lib.EFM_EXACT_STREAM):
+            assert L.efm_set_option(ctx, _lib.EFM_OPT_EXACT_FORM, form) == _lib.EFM_OK
+        assert L.efm_set_option(ctx, _lib.EFM_OPT_CHECKPOINT_EVERY, -1) == _lib.EFM_ERR_ARG
+        assert L.efm_set_option(ctx, _lib.EFM_OPT_CHECKPOINT_EVERY, 0) == _lib.EFM_OK  # automatic
+        assert L.efm_set_option(ctx, _lib.EFM_OPT_CHECKPOINT_EVERY, 25) == _lib.EFM_OK
         assert L.efm_smooth_mask(None, None, 1, 1, 1, 1.0, 0, 0, None) == _lib.EFM_ERR_ARG
         assert L.efm_lbfgs_history(None, None, None, None, 1, 0, 0, None) == _lib.EFM_ERR_ARG
     finally:

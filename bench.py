@@ -16,6 +16,10 @@ forward steps, nt-1 adjoint steps and nt-1 reverse rebuild steps.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload W]
 
+At N = 1 the line also carries ``batched``: the throughput of one sweep over 48 seeded
+instances of different grids in planned sub-batches (``batchbench.run``, uneven workload),
+reported beside the headline and not part of ``value`` (``--no-batched`` skips it).
+
 With N > 1 (torchrun, one rank per GPU) every rank runs its own shot (weak scaling) and
 the gradients and misfits are summed with one NCCL all-reduce per step -- the exchange
 the reference does with MPI Send/Recv + reduce (mainPropElastic3D_MT.py:2425-2475).
@@ -53,6 +57,8 @@ def parse():
                    help="back-to-back launches per kernel kind for the per-kernel times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-batched", action="store_true",
+                   help="skip the uneven-batch throughput reported beside the headline")
     p.add_argument("--no-graph", action="store_true",
                    help="launch the time loops step by step instead of replaying CUDA graphs")
     p.add_argument("--no-tune", action="store_true",
@@ -476,6 +482,15 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(args)
 
+    # Beside the headline (not part of value): one sweep of 48 seeded instances of different
+    # grids (64^3 .. 160x160x96), 1-4 sources each, in planned sub-batches, one launch per
+    # half-step -- forward + misfit + imaging gradient of all, CUDA events, after one warm-up.
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        from elastic_fm_vp_vs_rho_b200 import batchbench
+        batched = batchbench.run(argparse.Namespace(workload="uneven", n=48, steps=1, warmup=1,
+                                                    budget_gb=0.0, shots=32, nx=200, ny=200, nz=100))
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -487,7 +502,8 @@ def main():
                     time_loop="step launches" if args.no_graph else
                     "CUDA graph per time loop (captured once, replayed)"),
                 "gpu_launches": gpu_launches,
-                "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
+                "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "batched": batched}
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:

@@ -254,3 +254,42 @@ def test_autograd_function_velocity_gradients(case, oracle_grad, cuda):
     assert rel_err(vs.grad.cpu().numpy(), gvs) < TOL_EXACT
     assert rel_err(rho.grad.cpu().numpy(), grr) < TOL_EXACT
     assert rel_err(mt.grad.cpu().numpy().ravel(), gmt) < TOL_EXACT
+
+
+@pytest.mark.gpu
+def test_exact_stream_form_matches_two_pass_form_on_bench_grid(cuda):
+    """The plane-streaming transposes against the two-pass form on the 256 x 256 x 128 grid of
+    the bench workload (one shot, 240 steps: 128 tiles per plane, full y-chunk waves), with
+    the automatic checkpoint interval for the streaming form and 40-step segments for the
+    two-pass one; the exact MT gradient and the model gradients agree to 1e-6."""
+    from elastic_fm_vp_vs_rho_b200 import ShotBatch, _lib
+    w = configs.learned_fwi_shot(nt=240)
+    s = w.shots[0]
+    cp = configs.cpml_profiles(w.fq, w.dt, w.dx, w.lenpml, float(max(w.vp.max(), w.vp0.max())),
+                               w.nx, w.ny, w.nz)
+    lam0, mu0 = configs.lame_from_velocity(w.vp0, w.vs0, w.rho0)
+    lam, mu = configs.lame_from_velocity(w.vp, w.vs, w.rho)
+    obs_b = ShotBatch()
+    kw = dict(nx=w.nx, ny=w.ny, nz=w.nz, lenpml=w.lenpml, dx=w.dx, dt=w.dt, nt=w.nt, cpml=cp,
+              wavelet=configs.ricker(w.fq, w.dt, w.nt), src=[[s.sx, s.sy, s.sz]], mt=[s.mt],
+              rec=np.stack([s.rec_x, s.rec_y, s.rec_z], axis=1))
+    obs_b.add(lam=lam, mu=mu, rho=w.rho, **kw)
+    obs = obs_b.forward().clone()
+    obs_b.close()
+    out = {}
+    for form, K in ((_lib.EFM_EXACT_TWO_PASS, 40), (_lib.EFM_EXACT_STREAM, 0)):
+        b = ShotBatch()
+        b.add(lam=lam0, mu=mu0, rho=w.rho0, **kw)
+        b.set_option(_lib.EFM_OPT_EXACT_FORM, form)
+        b.set_option(_lib.EFM_OPT_CHECKPOINT_EVERY, K)
+        mod = b.forward(checkpoints=True)
+        res, _ = b.residual_misfit(mod, obs)
+        g, m = b.gradient(res, exact=True, mt=True)
+        b.status()
+        out[form] = (b.grad_view(g, 0).cpu().numpy(), m[0, 0].cpu().numpy())
+        b.close()
+    (g0, m0), (g1, m1) = out[_lib.EFM_EXACT_TWO_PASS], out[_lib.EFM_EXACT_STREAM]
+    for i in range(3):
+        assert np.abs(g0[i]).max() > 0
+        assert rel_err(g1[i], g0[i]) < 1e-6, i
+    assert rel_err(m1, m0) < 1e-6

@@ -118,6 +118,7 @@ SIGNATURES = {
                                          ctypes.c_size_t, _P]),
     "efm_conv3d_status": (_I, [_P]),
     "efm_conv3d_set_grouped_loads": (None, [_I]),
+    "efm_conv3d_set_swizzled_loads": (None, [_I]),
 }
 
 _lock = threading.Lock()

@@ -24,10 +24,17 @@
 // weight gradient  (efm_conv_wgrad_kernel)
 //   GEMM: M = (kd, kh, ci) rows -- 128 / cin (kd, kh) pairs of cin channels per tile --,
 //   N = cout, K = voxels.  Both operands are MN-major slabs read straight from the
-//   channels-last volumes (8 channels x 128 or 136 voxels per TMA box); the three kw taps
-//   again come from start-address shifts of one 136-row input slab, accumulated in three
-//   TMEM column ranges.  Blocks split K; partial sums go to a workspace and a second kernel
-//   reduces them in a fixed order (deterministic).
+//   channels-last volumes; the three kw taps again come from start-address shifts of one
+//   136-row input slab, accumulated in three TMEM column ranges.  Default (SW): one TMA box
+//   per input row holding all cin channels of 136 voxels (a 2 cin-byte row per voxel, 32 /
+//   64 / 128-byte swizzle) and one for the gradient row (128 voxels x cout channels), in
+//   the swizzled canonical layouts -- a few wide L2 requests per row instead of one 16-byte
+//   request per voxel and 8-channel slab.  Otherwise 8-channel x 136-voxel slabs without
+//   swizzle (efm_conv3d_set_swizzled_loads(0)).  The pair slots past the ninth (the last
+//   tile always has one) are never loaded: they hold ones, so their accumulator rows sum
+//   the output gradient over the voxels -- the bias gradient, at no extra pass.  Blocks
+//   split K; partial sums go to a workspace and a second kernel reduces them in a fixed
+//   order (deterministic).
 //
 // Every mbarrier wait is bounded; a block that gives up sets the error word, waits (bounded)
 // for its own TMA loads and MMAs in flight, frees its TMEM and returns.
@@ -62,6 +69,7 @@ constexpr int WG_K = 128;                  // voxels per weight-gradient K chunk
 constexpr int WG_AROWS = 136;              // x0-4 .. x0+131
 constexpr int WG_ASLAB = WG_AROWS * 16;    // 2176
 constexpr int WG_BSLAB = WG_K * 16;        // 2048
+constexpr int WG_YB = 8;                   // weight-gradient units walk y in bands of 8 planes
 
 __device__ unsigned int g_conv_err;
 
@@ -337,24 +345,47 @@ efm_conv_fwd_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_const
 
 // ------------------------------------------------------------------------ weight gradient
 // partial[split][q][kw][128][COUT]: rows (local pair, ci) of M tile q.
-template <int CIN, int COUT>
+template <int CIN, int COUT, bool SW>
 __global__ void __launch_bounds__(CV_THREADS, 1)
 efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_dy,
                       int nx, int ny, int nz, float *__restrict__ partial, int grouped) {
     constexpr int NPAIR = 128 / CIN;               // (kd, kh) pairs per M tile
     constexpr int NGI = CIN / 8, NGO = COUT / 8;
-    constexpr int ASTAGE = NPAIR * NGI * WG_ASLAB;  // 16 slabs
-    constexpr int BSTAGE = NGO * WG_BSLAB;
-    constexpr int STAGE = ASTAGE + BSTAGE;
+    constexpr int AROWB = 2 * CIN, BROWB = 2 * COUT;  // swizzled: bytes per voxel row
+    constexpr int ASLAB = SW ? (WG_AROWS * AROWB + 1023) / 1024 * 1024 : NGI * WG_ASLAB;
+    constexpr int ASTAGE = NPAIR * ASLAB;           // one slab (set) per pair
+    constexpr int BSTAGE = SW ? WG_K * BROWB : NGO * WG_BSLAB;
+    constexpr int STAGE = ASTAGE + BSTAGE;          // a multiple of 1024 bytes when SW
+    // bytes each stage receives: the loaded pairs (9 - q NPAIR in the last tile) and the gradient
+    const int nload = min(NPAIR, 9 - (int)blockIdx.y * NPAIR);
+    const uint32_t TX = nload * (SW ? WG_AROWS * AROWB : ASLAB) + (SW ? WG_K * BROWB : BSTAGE);
+    constexpr uint32_t LAY_A = CIN == 16 ? 6u : CIN == 32 ? 4u : 2u;  // 32 / 64 / 128-byte swizzle
+    constexpr uint32_t LAY_B = COUT == 16 ? 6u : COUT == 32 ? 4u : 2u;
     constexpr uint32_t IDESC = efm_idesc_bf16(128, COUT, true, true);
     constexpr uint32_t NCOLS = 3 * COUT <= 32 ? 32 : 3 * COUT <= 64 ? 64 : 3 * COUT <= 128 ? 128 : 256;
-    extern __shared__ __align__(1024) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // the swizzle patterns are anchored at 1024-byte boundaries (the launch adds 1 KB of slack)
+    unsigned char *smem = smem_raw + ((1024u - (efm_smem_addr(smem_raw) & 1023u)) & 1023u);
     __shared__ Sync S;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int q = blockIdx.y, split = blockIdx.x, nsplit = gridDim.x;
     const int xc = (nx + WG_K - 1) / WG_K;
-    const int64_t units = (int64_t)xc * nz * ny;
+    // units (x chunk, y, z) in the order x chunk, y within a band of WG_YB planes, z, band: an
+    // input row enters the units of its three y neighbours and three z neighbours within
+    // about 3 WG_YB units, so it is re-read from L2 while it is still there (units past ny
+    // load zero rows and add nothing)
+    const int64_t units = (int64_t)xc * nz * ((ny + WG_YB - 1) / WG_YB * WG_YB);
     const int64_t u0 = units * split / nsplit, u1 = units * (split + 1) / nsplit;
+    // the unloaded pair slots of every stage: ones (BF16 0x3F80), written once through the
+    // generic proxy and fenced for the MMAs' async-proxy reads before the set-up barrier
+    if (nload < NPAIR) {
+        const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+        for (int st = 0; st < CV_STAGES; ++st) {
+            uint4 *p = reinterpret_cast<uint4 *>(smem + st * STAGE + nload * ASLAB);
+            for (int i = threadIdx.x; i < (NPAIR - nload) * ASLAB / 16; i += blockDim.x) p[i] = ones;
+        }
+        efm_fence_async_smem();
+    }
     cv_setup(S, 128, NCOLS, CV_STAGES);
     volatile int *abort = &S.abort;
     bool mma_issued = false;
@@ -368,22 +399,29 @@ efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_con
         bool issued[CV_STAGES] = {};
         bool ok = true;
         for (int64_t u = u0; u < u1; ++u) {
-            const int x0 = (int)(u % xc) * WG_K, z = (int)((u / xc) % nz), y = (int)(u / ((int64_t)xc * nz));
+            const int x0 = (int)(u % xc) * WG_K;
+            const int64_t r = u / xc;
+            const int z = (int)((r / WG_YB) % nz);
+            const int y = (int)((r / WG_YB / nz) * WG_YB + r % WG_YB);
             if (!cv_wait(&S.empty[st], ph ^ 1u, abort)) { ok = false; break; }
-            efm_mbar_expect_tx(&S.full[st], STAGE);
+            efm_mbar_expect_tx(&S.full[st], TX);
             unsigned char *dst = smem + st * STAGE;
             for (int lp = 0; lp < NPAIR; ++lp) {
-                const int pi = q * NPAIR + lp;  // (kd, kh) = (pi / 3, pi % 3); pi > 8: zero rows
-                const int zz = pi < 9 ? z + pi % 3 - 1 : -64;
-                const int yy = pi < 9 ? y + pi / 3 - 1 : -64;
-                if (grouped)
-                    efm_tma_load_5d(dst + lp * NGI * WG_ASLAB, &tm_x, &S.full[st], 0, x0 - 4, zz, yy, 0);
+                const int pi = q * NPAIR + lp;  // (kd, kh) = (pi / 3, pi % 3); pi > 8: the ones
+                if (pi >= 9) break;
+                const int zz = z + pi % 3 - 1, yy = y + pi / 3 - 1;
+                if (SW)
+                    efm_tma_load_4d(dst + lp * ASLAB, &tm_x, &S.full[st], 0, x0 - 4, zz, yy);
+                else if (grouped)
+                    efm_tma_load_5d(dst + lp * ASLAB, &tm_x, &S.full[st], 0, x0 - 4, zz, yy, 0);
                 else
                     for (int g = 0; g < NGI; ++g)
-                        efm_tma_load_4d(dst + (lp * NGI + g) * WG_ASLAB, &tm_x, &S.full[st], 8 * g,
+                        efm_tma_load_4d(dst + lp * ASLAB + g * WG_ASLAB, &tm_x, &S.full[st], 8 * g,
                                         x0 - 4, zz, yy);
             }
-            if (grouped)
+            if (SW)
+                efm_tma_load_4d(dst + ASTAGE, &tm_dy, &S.full[st], 0, x0, z, y);
+            else if (grouped)
                 efm_tma_load_5d(dst + ASTAGE, &tm_dy, &S.full[st], 0, x0, z, y, 0);
             else
                 for (int g = 0; g < NGO; ++g)
@@ -404,13 +442,18 @@ efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_con
             if (!cv_wait(&S.full[st], ph, abort)) { ok = false; break; }
             efm_tc_fence_after();
             const uint32_t a0 = base + st * STAGE, b0 = a0 + ASTAGE;
-            const uint64_t adesc = efm_sdesc(a0, 128, WG_ASLAB), bdesc = efm_sdesc(b0, 128, WG_BSLAB);
+            // rows of 16 bytes (8 channels) unswizzled, of 2 cin / 2 cout bytes swizzled; a
+            // K step is 16 voxel rows, the kw taps start 3, 4, 5 rows into the input slab
+            constexpr uint32_t RA = SW ? AROWB : 16, RB = SW ? BROWB : 16;
+            const uint64_t adesc = SW ? efm_sdesc_sw(a0, ASLAB, 8 * RA, LAY_A) : efm_sdesc(a0, 128, WG_ASLAB);
+            const uint64_t bdesc = SW ? efm_sdesc_sw(b0, BSTAGE, 8 * RB, LAY_B) : efm_sdesc(b0, 128, WG_BSLAB);
+            // K steps outer, kw taps inner: consecutive MMAs write different accumulators
 #pragma unroll
-            for (int kw = 0; kw < 3; ++kw) {
+            for (int j = 0; j < WG_K / 16; ++j) {
 #pragma unroll
-                for (int j = 0; j < WG_K / 16; ++j) {
-                    const uint64_t a = adesc + (uint64_t)((256 * j + (kw + 3) * 16) >> 4);
-                    const uint64_t b = bdesc + (uint64_t)((256 * j) >> 4);
+                for (int kw = 0; kw < 3; ++kw) {
+                    const uint64_t a = adesc + (uint64_t)((16 * RA * j + (kw + 3) * RA) >> 4);
+                    const uint64_t b = bdesc + (uint64_t)((16 * RB * j) >> 4);
                     efm_mma_bf16(S.tmem + kw * COUT, a, b, IDESC, (u != u0 || j != 0) ? 1u : 0u);
                 }
             }
@@ -453,11 +496,20 @@ efm_conv_wgrad_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_con
     cv_teardown(S, NCOLS, mma_issued);
 }
 
-// dw[t][co][ci] = sum over splits (fixed order) of the partial rows; t = 3 pi + kw.
+// dw[t][co][ci] = sum over splits (fixed order) of the partial rows; t = 3 pi + kw.  db[co]
+// (when db is not null) = the same sum of the first ones row (pair slot 9, channel 0, kw 1).
 __global__ void efm_conv_wgrad_reduce(const float *__restrict__ partial, int nsplit, int nq,
-                                      int cin, int cout, float *__restrict__ dw) {
+                                      int cin, int cout, float *__restrict__ dw,
+                                      float *__restrict__ db) {
     const int n = 27 * cout * cin;
     const int npair = 128 / cin;
+    if (db != nullptr && blockIdx.x == 0 && (int)threadIdx.x < cout) {
+        const int co = threadIdx.x, qq = 9 / npair, row = (9 % npair) * cin;
+        double s = 0.0;
+        for (int sp = 0; sp < nsplit; ++sp)
+            s += partial[((((int64_t)sp * nq + qq) * 3 + 1) * 128 + row) * cout + co];
+        db[co] = (float)s;
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int ci = i % cin, co = (i / cin) % cout, t = i / (cin * cout);
         const int pi = t / 3, kw = t % 3, qq = pi / npair, lp = pi % npair;
@@ -467,33 +519,6 @@ __global__ void efm_conv_wgrad_reduce(const float *__restrict__ partial, int nsp
             s += partial[((((int64_t)sp * nq + qq) * 3 + kw) * 128 + row) * cout + co];
         dw[i] = (float)s;
     }
-}
-
-// db[co] = sum over voxels of dy[., co]: per-block partial sums, then a fixed-order total.
-__global__ void efm_conv_bias_partial(const __nv_bfloat16 *__restrict__ dy, int64_t nvox, int cout,
-                                      float *__restrict__ part) {
-    // block b, thread (c, r): channel c = threadIdx.x % cout, voxel lane r = threadIdx.x / cout
-    const int c = threadIdx.x % cout, r = threadIdx.x / cout, nr = blockDim.x / cout;
-    float s = 0.f;
-    for (int64_t v = (int64_t)blockIdx.x * nr + r; v < nvox; v += (int64_t)gridDim.x * nr)
-        s += __bfloat162float(dy[v * cout + c]);
-    extern __shared__ float red[];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    if (r == 0) {
-        float t = 0.f;
-        for (int k = 0; k < nr; ++k) t += red[k * cout + c];
-        part[(int64_t)blockIdx.x * cout + c] = t;
-    }
-}
-
-__global__ void efm_conv_bias_final(const float *__restrict__ part, int nblocks, int cout,
-                                    float *__restrict__ db) {
-    const int c = threadIdx.x;
-    if (c >= cout) return;
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += part[(int64_t)b * cout + c];
-    db[c] = (float)s;
 }
 
 // fp32 [27][cout][cin] -> bf16 forward weights and bf16 mirrored transpose [27][cin][cout]
@@ -558,6 +583,26 @@ int map_volume(CUtensorMap *m, const void *base, const efm_conv_desc *d, int c, 
     return EFM_OK;
 }
 
+// channels-last BF16 volume (ny, nz, nx, c); box (all c channels, rows along x, 1, 1) with the
+// 32 / 64 / 128-byte swizzle of a 2c-byte row (c = 16 / 32 / 64)
+int map_volume_swizzled(CUtensorMap *m, const void *base, const efm_conv_desc *d, int c, int rows) {
+    auto enc = conv_encoder();
+    if (!enc) return efm_internal_fail(EFM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)d->nx, (cuuint64_t)d->nz, (cuuint64_t)d->ny};
+    cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)c * 2 * d->nx,
+                             (cuuint64_t)c * 2 * d->nx * d->nz};
+    cuuint32_t box[4] = {(cuuint32_t)c, (cuuint32_t)rows, 1, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUtensorMapSwizzle sw = c == 16 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                  : c == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides,
+                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return efm_internal_fail(EFM_ERR_CUDA, ("tensor map (swizzled volume) failed: " + std::to_string((int)r)).c_str());
+    return EFM_OK;
+}
+
 // weights [27][cout][cin] BF16 seen as (cin, cout, kw, 3 kd + kh); box (8, cout, 1, 3): the
 // three kh taps of one (kd, kw) as consecutive rows
 int map_weights(CUtensorMap *m, const void *base, int cin, int cout) {
@@ -578,6 +623,8 @@ int map_weights(CUtensorMap *m, const void *base, int cin, int cout) {
 
 // 1: one 5-D TMA copy per slab set when the driver accepts the map; 0: per-group copies
 int g_grouped_ok = 1;
+// weight gradient: 1 = swizzled full-channel rows (default), 0 = 8-channel slabs
+int g_wgrad_swizzled = 1;
 
 bool chan_ok(int c) { return c == 16 || c == 32 || c == 64; }
 
@@ -633,7 +680,7 @@ int dispatch_fwd(int cin, int cout, const efm_conv_desc *d, const CUtensorMap &t
 }
 
 int wgrad_splits(const efm_conv_desc *d, int nq) {
-    const int64_t units = (int64_t)((d->nx + WG_K - 1) / WG_K) * d->nz * d->ny;
+    const int64_t units = (int64_t)((d->nx + WG_K - 1) / WG_K) * d->nz * ((d->ny + WG_YB - 1) / WG_YB * WG_YB);
     int64_t s = num_sms() / nq;  // one wave of single-block SMs
     if (s > units) s = units;
     return (int)(s < 1 ? 1 : s);
@@ -641,13 +688,14 @@ int wgrad_splits(const efm_conv_desc *d, int nq) {
 
 int wgrad_nq(int cin) { return (9 + 128 / cin - 1) / (128 / cin); }
 
-template <int CIN, int COUT>
+template <int CIN, int COUT, bool SW>
 int launch_wgrad(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMap &tdy, float *part,
                  int nsplit, int grouped, cudaStream_t s) {
-    constexpr int stage = (128 / CIN) * (CIN / 8) * WG_ASLAB + (COUT / 8) * WG_BSLAB;
-    const int smem_need = CV_STAGES * stage;
+    constexpr int aslab = SW ? (WG_AROWS * 2 * CIN + 1023) / 1024 * 1024 : (CIN / 8) * WG_ASLAB;
+    constexpr int stage = (128 / CIN) * aslab + (SW ? WG_K * 2 * COUT : (COUT / 8) * WG_BSLAB);
+    const int smem_need = CV_STAGES * stage + 1024;  // + slack for the 1024-byte alignment
     const int smem = smem_need > CV_MIN_SMEM ? smem_need : CV_MIN_SMEM;
-    auto k = efm_conv_wgrad_kernel<CIN, COUT>;
+    auto k = efm_conv_wgrad_kernel<CIN, COUT, SW>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
     dim3 grid(nsplit, wgrad_nq(CIN));
@@ -656,7 +704,6 @@ int launch_wgrad(const efm_conv_desc *d, const CUtensorMap &tx, const CUtensorMa
     return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
 }
 
-constexpr int BIAS_BLOCKS = 296;
 
 }  // namespace
 
@@ -712,7 +759,7 @@ size_t efm_conv3d_wgrad_workspace(const efm_conv_desc *d) {
     if (check_desc(d)) return 0;
     const int nq = wgrad_nq(d->cin);
     const size_t part = (size_t)wgrad_splits(d, nq) * nq * 3 * 128 * d->cout * sizeof(float);
-    return part + (size_t)BIAS_BLOCKS * d->cout * sizeof(float);
+    return part;
 }
 
 int efm_conv3d_backward_weights(const efm_conv_desc *d, const void *x, const void *dy, float *dw,
@@ -725,33 +772,36 @@ int efm_conv3d_backward_weights(const efm_conv_desc *d, const void *x, const voi
         return efm_internal_fail(EFM_ERR_ARG, "buffers must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
     CUtensorMap tx, tdy;
-    const int grouped = g_grouped_ok && map_volume_grouped(&tx, x, d, d->cin, WG_AROWS) &&
+    const bool sw = g_wgrad_swizzled != 0;
+    const int grouped = !sw && g_grouped_ok && map_volume_grouped(&tx, x, d, d->cin, WG_AROWS) &&
                         map_volume_grouped(&tdy, dy, d, d->cout, WG_K);
-    if (!grouped && (rc = map_volume(&tx, x, d, d->cin, WG_AROWS))) return rc;
-    if (!grouped && (rc = map_volume(&tdy, dy, d, d->cout, WG_K))) return rc;
+    if (sw) {
+        if ((rc = map_volume_swizzled(&tx, x, d, d->cin, WG_AROWS))) return rc;
+        if ((rc = map_volume_swizzled(&tdy, dy, d, d->cout, WG_K))) return rc;
+    } else if (!grouped) {
+        if ((rc = map_volume(&tx, x, d, d->cin, WG_AROWS))) return rc;
+        if ((rc = map_volume(&tdy, dy, d, d->cout, WG_K))) return rc;
+    }
     const int nq = wgrad_nq(d->cin), nsplit = wgrad_splits(d, nq);
     float *part = static_cast<float *>(workspace);
     rc = EFM_ERR_ARG;
-#define EFM_WG_CASE(A, B) \
-    if (d->cin == A && d->cout == B) rc = launch_wgrad<A, B>(d, tx, tdy, part, nsplit, grouped, s);
+#define EFM_WG_CASE(A, B)                                                                       \
+    if (d->cin == A && d->cout == B)                                                            \
+        rc = sw ? launch_wgrad<A, B, true>(d, tx, tdy, part, nsplit, grouped, s)                \
+                : launch_wgrad<A, B, false>(d, tx, tdy, part, nsplit, grouped, s);
     EFM_WG_CASE(16, 16) EFM_WG_CASE(16, 32) EFM_WG_CASE(16, 64)
     EFM_WG_CASE(32, 16) EFM_WG_CASE(32, 32) EFM_WG_CASE(32, 64)
     EFM_WG_CASE(64, 16) EFM_WG_CASE(64, 32)
 #undef EFM_WG_CASE
     if (rc) return rc;
-    efm_conv_wgrad_reduce<<<64, 256, 0, s>>>(part, nsplit, nq, d->cin, d->cout, dw);
-    if (db) {
-        float *bp = part + (size_t)nsplit * nq * 3 * 128 * d->cout;
-        const int64_t nvox = (int64_t)d->nx * d->ny * d->nz;
-        efm_conv_bias_partial<<<BIAS_BLOCKS, 256, 256 * sizeof(float), s>>>(
-            static_cast<const __nv_bfloat16 *>(dy), nvox, d->cout, bp);
-        efm_conv_bias_final<<<1, 64, 0, s>>>(bp, BIAS_BLOCKS, d->cout, db);
-    }
+    efm_conv_wgrad_reduce<<<64, 256, 0, s>>>(part, nsplit, nq, d->cin, d->cout, dw, db);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? EFM_OK : efm_internal_fail(EFM_ERR_CUDA, cudaGetErrorString(e));
 }
 
 void efm_conv3d_set_grouped_loads(int enable) { g_grouped_ok = enable != 0; }
+
+void efm_conv3d_set_swizzled_loads(int enable) { g_wgrad_swizzled = enable != 0; }
 
 int efm_conv3d_status(void *stream) {
     cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);

@@ -9,7 +9,8 @@
 // and its LBO the distance between core matrices adjacent along K.  When a slab keeps its
 // 16-byte rows contiguous (SBO = 128 for K-major, LBO = 128 for MN-major) the row index is
 // linear in the address, so moving the start address by 16 bytes shifts the operand by one
-// row -- the convolution kernels use this for the +-1 tap offsets along x.
+// row -- the convolution kernels use this for the +-1 tap offsets along x.  The weight
+// gradient's full-channel rows use the swizzled MN-major layouts (efm_sdesc_sw).
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -25,6 +26,18 @@ __device__ __forceinline__ uint64_t efm_sdesc(uint32_t saddr, uint32_t lbo, uint
     d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1 << 46;
     return d;
+}
+
+// The same for a swizzled canonical layout (layout type in bits 61-63: 6 = 32-byte, 4 =
+// 64-byte, 2 = 128-byte swizzle).  For an MN-major operand the rows (one K index each) are
+// the swizzle width (32 / 64 / 128 bytes = 16 / 32 / 64 BF16 along M/N) apart; LBO is the byte
+// distance between such M/N blocks and SBO the distance between groups of 8 rows along K.
+// The XOR pattern is taken from the absolute address bits (the same function the TMA
+// swizzle applies), so with the pattern anchored at a 1024-byte boundary (base offset 0) the
+// start address may move by whole rows: the row shift of the kw taps works as unswizzled.
+__device__ __forceinline__ uint64_t efm_sdesc_sw(uint32_t saddr, uint32_t lbo, uint32_t sbo,
+                                                 uint32_t layout) {
+    return efm_sdesc(saddr, lbo, sbo) | ((uint64_t)(layout & 7u) << 61);
 }
 
 // Instruction descriptor of tcgen05.mma.kind::f16 with BF16 A and B and an FP32

@@ -396,6 +396,10 @@ EFM_API int efm_conv3d_status(void *stream);
 /* 1 (default): stage all 8-channel slabs of an input row with one TMA copy (a 5-D tensor
  * map) when the driver accepts that map; 0: one copy per slab.  Results are identical. */
 EFM_API void efm_conv3d_set_grouped_loads(int enable);
+/* Weight gradient: 1 (default) stages each input / gradient row as one TMA box of all its
+ * channels in the swizzled canonical layout; 0: as 8-channel slabs without swizzle (then
+ * efm_conv3d_set_grouped_loads applies).  Results are identical. */
+EFM_API void efm_conv3d_set_swizzled_loads(int enable);
 
 #ifdef __cplusplus
 }

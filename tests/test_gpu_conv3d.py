@@ -119,19 +119,22 @@ def test_weight_layout_roundtrip_and_unsupported_pairs():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cin,cout", [(32, 64), (64, 16)])
-def test_grouped_and_per_slab_loads_agree(cuda, cin, cout):
-    """One 5-D TMA copy per input row or one copy per 8-channel slab: identical results."""
+@pytest.mark.parametrize("cin,cout", [(32, 64), (64, 16), (16, 32), (64, 32), (32, 16)])
+def test_grouped_per_slab_and_swizzled_loads_agree(cuda, cin, cout):
+    """The operand staging variants give identical results: one 5-D TMA copy per input row or
+    one copy per 8-channel slab (all kernels), and, for the weight gradient, full-channel
+    rows in the swizzled layouts (default) or 8-channel slabs without swizzle."""
     import torch
     from elastic_fm_vp_vs_rho_b200 import _lib, conv3d
-    x, w, b = _data((3, 6, 40), cin, cout, 11)
+    x, w, b = _data((3, 6, 140), cin, cout, 11)
     g = torch.Generator().manual_seed(12)
-    dy = torch.randn((3, 6, 40, cout), generator=g).to(torch.bfloat16).cuda()
+    dy = torch.randn((3, 6, 140, cout), generator=g).to(torch.bfloat16).cuda()
     wb, wt = conv3d.prep_weights(w.cuda())
     L = _lib.load()
     outs = []
-    for grouped in (1, 0):
+    for grouped, sw in ((1, 1), (1, 0), (0, 0)):
         L.efm_conv3d_set_grouped_loads(grouped)
+        L.efm_conv3d_set_swizzled_loads(sw)
         try:
             _, yf = conv3d.forward(x.cuda(), wb, b.cuda(), relu=True, out_bf16=False, out_f32=True)
             dx = conv3d.backward_data(dy, wt, cin, relu_mask=x.cuda())
@@ -139,6 +142,8 @@ def test_grouped_and_per_slab_loads_agree(cuda, cin, cout):
             conv3d.status()
         finally:
             L.efm_conv3d_set_grouped_loads(1)
+            L.efm_conv3d_set_swizzled_loads(1)
         outs.append((yf.cpu(), dx.cpu(), dw.cpu(), db.cpu()))
-    for a, c in zip(*outs):
-        assert torch.equal(a, c)
+    for k in (1, 2):
+        for a, c in zip(outs[0], outs[k]):
+            assert torch.equal(a, c)

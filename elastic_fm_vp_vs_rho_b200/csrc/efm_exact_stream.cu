@@ -149,7 +149,9 @@ __device__ __forceinline__ float xs_g(float a, bool slab, float u, float p) {
 // The x / z part of a cell, fixed for the block's whole march: its offset inside a plane, the
 // domain tests, slab membership and CPML coefficients of the x and z families, and its
 // memory-variable offsets inside a plane of the x and z slab families.
-enum { XS_INXZ = 1, XS_GDXZ = 2, XS_SX = 4, XS_SZ = 8 };
+// XS_WSX / XS_WSZ: some lane of the warp has its cell in the x / z slab (the memory-variable
+// code of that family is skipped by whole warps otherwise)
+enum { XS_INXZ = 1, XS_GDXZ = 2, XS_SX = 4, XS_SZ = 8, XS_WSX = 16, XS_WSZ = 32 };
 
 struct XsCol {
     int off;   // z * nx + x
@@ -166,7 +168,8 @@ __device__ __forceinline__ XsCol xs_col(const XsC &C, int x, int z) {
     const bool gdx = x >= EFM_HS && x < nx - 1, gdz = z >= EFM_HS && z < nz - 1;
     const bool sx = x < W || x >= nx - W, sz = z >= nz - W;
     k.flags = (inx && inz ? XS_INXZ : 0) | (gdx && gdz ? XS_GDXZ : 0) | (sx ? XS_SX : 0) |
-              (sz ? XS_SZ : 0);
+              (sz ? XS_SZ : 0) | (__any_sync(0xffffffffu, sx) ? XS_WSX : 0) |
+              (__any_sync(0xffffffffu, sz) ? XS_WSZ : 0);
     k.pxo = z * 2 * W + (x < W ? x : x - (nx - 2 * W));
     const bool xin = x >= 0 && x < nx, zin = z >= 0 && z < nz;
     k.ax = xin ? __ldg(C.cpml + x) : 0.f;
@@ -236,12 +239,22 @@ struct XsPsi {
 __device__ __forceinline__ void xs_psi_load(const XsPsiPtr &Q, const XsRow &R, const XsCol &k,
                                             XsPsi &s) {
     const bool sx = k.flags & XS_SX, sz = k.flags & XS_SZ;
-    const int ix = xs_ix(R, k), iy = xs_iy(R, k), iz = xs_iz(R, k);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        s.x[q] = sx ? Q.x[q * Q.sx + ix] : 0.f;
-        s.y[q] = R.sy ? Q.y[q * Q.sy + iy] : 0.f;
-        s.z[q] = sz ? Q.z[q * Q.sz + iz] : 0.f;
+    for (int q = 0; q < 3; ++q) s.x[q] = s.y[q] = s.z[q] = 0.f;
+    if (k.flags & XS_WSX) {  // warp-uniform
+        const int ix = xs_ix(R, k);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s.x[q] = sx ? Q.x[q * Q.sx + ix] : 0.f;
+    }
+    if (R.sy) {  // block-uniform
+        const int iy = xs_iy(R, k);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s.y[q] = Q.y[q * Q.sy + iy];
+    }
+    if (k.flags & XS_WSZ) {
+        const int iz = xs_iz(R, k);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s.z[q] = sz ? Q.z[q * Q.sz + iz] : 0.f;
     }
 }
 
@@ -250,12 +263,22 @@ __device__ __forceinline__ void xs_psi_store(const XsPsiPtr &Q, const XsRow &R, 
                                              const XsPsi &s, const float (&ux)[3],
                                              const float (&uy)[3], const float (&uz)[3]) {
     const bool sx = k.flags & XS_SX, sz = k.flags & XS_SZ;
-    const int ix = xs_ix(R, k), iy = xs_iy(R, k), iz = xs_iz(R, k);
+    if (k.flags & XS_WSX) {
+        const int ix = xs_ix(R, k);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        if (sx) Q.ox[q * Q.sx + ix] = k.bx * (s.x[q] + ux[q]);
-        if (R.sy) Q.oy[q * Q.sy + iy] = R.by * (s.y[q] + uy[q]);
-        if (sz) Q.oz[q * Q.sz + iz] = k.bz * (s.z[q] + uz[q]);
+        for (int q = 0; q < 3; ++q)
+            if (sx) Q.ox[q * Q.sx + ix] = k.bx * (s.x[q] + ux[q]);
+    }
+    if (R.sy) {
+        const int iy = xs_iy(R, k);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) Q.oy[q * Q.sy + iy] = R.by * (s.y[q] + uy[q]);
+    }
+    if (k.flags & XS_WSZ) {
+        const int iz = xs_iz(R, k);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (sz) Q.oz[q * Q.sz + iz] = k.bz * (s.z[q] + uz[q]);
     }
 }
 

@@ -18,8 +18,11 @@
 // sums differs (the mu gradient's four shear products of a pair are added two by two), and
 // the stress transpose's three reciprocals (of 3 lambda + 2 mu, mu and mu^2) use the hardware
 // reciprocal (relative error ~1 ulp) as the forward kernels' harmonic means do.
-// Plain coalesced loads (one warp = 32 cells of a row): the block waits for nothing but
-// its own loads and the per-plane barrier.
+// Plain coalesced loads (one warp = 32 cells of a row), all of a plane's loads -- its own
+// cells', its halo cell's and the outputs of the plane being gathered -- issued before any
+// store, so a thread waits one memory latency per plane; the x / z parts of every index,
+// domain test and CPML coefficient are computed once per thread (XsCol), the y parts once per
+// plane (XsRow).  The block waits for nothing but its own loads and the per-plane barrier.
 #include <cuda_runtime.h>
 #include <stdint.h>
 

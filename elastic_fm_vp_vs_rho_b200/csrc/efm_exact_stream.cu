@@ -865,16 +865,22 @@ int xs_smem_bytes(int nf) {
     return 3 * nf * XsGeom<ROWS>::PL * (int)sizeof(float);
 }
 
-// Allow the kernels' dynamic shared memory (above the 48 KB default) on the current device.
+// Allow the kernels' dynamic shared memory (above the 48 KB default) on the current device,
+// once per device.
 template <int ROWS>
 cudaError_t xs_attrs() {
-    cudaError_t e = cudaFuncSetAttribute(efm_exact_vt_stream<ROWS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         xs_smem_bytes<ROWS>(VT_NF));
+    static bool done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(efm_exact_vt_stream<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             xs_smem_bytes<ROWS>(VT_NF));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(efm_exact_st_stream<ROWS>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  xs_smem_bytes<ROWS>(ST_NF));
+    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
 }
 

@@ -153,8 +153,10 @@ __device__ __forceinline__ float xs_g(float a, bool slab, float u, float p) {
 // domain tests, slab membership and CPML coefficients of the x and z families, and its
 // memory-variable offsets inside a plane of the x and z slab families.
 // XS_WSX / XS_WSZ: some lane of the warp has its cell in the x / z slab (the memory-variable
-// code of that family is skipped by whole warps otherwise)
-enum { XS_INXZ = 1, XS_GDXZ = 2, XS_SX = 4, XS_SZ = 8, XS_WSX = 16, XS_WSZ = 32 };
+// code of that family is skipped by whole warps otherwise); XS_WAX / XS_WAZ: some lane has
+// a nonzero CPML a of that family (else the mixing (1 + a) u + a psibar is u for the warp)
+enum { XS_INXZ = 1, XS_GDXZ = 2, XS_SX = 4, XS_SZ = 8, XS_WSX = 16, XS_WSZ = 32, XS_WAX = 64,
+       XS_WAZ = 128 };
 
 struct XsCol {
     int off;   // z * nx + x
@@ -178,6 +180,8 @@ __device__ __forceinline__ XsCol xs_col(const XsC &C, int x, int z) {
     k.ax = xin ? __ldg(C.cpml + x) : 0.f;
     k.bx = xin ? __ldg(C.cpml + nx + x) : 0.f;
     k.az = zin ? __ldg(C.cpml + 2 * nx + 2 * C.ny + z) : 0.f;
+    k.flags |= (__any_sync(0xffffffffu, k.ax != 0.f) ? XS_WAX : 0) |
+               (__any_sync(0xffffffffu, k.az != 0.f) ? XS_WAZ : 0);
     k.bz = zin ? __ldg(C.cpml + 2 * nx + 2 * C.ny + nz + z) : 0.f;
     return k;
 }
@@ -343,10 +347,20 @@ __device__ __forceinline__ void vt_form(float kdt, const XsPsiPtr &Q, const XsRo
     const float ux[3] = {u[0], u[1], u[2]}, uy[3] = {u[1], u[0], u[2]}, uz[3] = {u[2], u[0], u[1]};
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        g[j] = xs_g(k.ax, sx, ux[j], r.p.x[j]);
-        g[3 + j] = xs_g(R.ay, R.sy, uy[j], r.p.y[j]);
-        g[6 + j] = xs_g(k.az, sz, uz[j], r.p.z[j]);
+        g[j] = ux[j];
+        g[3 + j] = uy[j];
+        g[6 + j] = uz[j];
     }
+    // the CPML mixing, skipped by warps (x, z) or planes (y) where every a is zero
+    if (k.flags & XS_WAX)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) g[j] = xs_g(k.ax, sx, ux[j], r.p.x[j]);
+    if (R.ay != 0.f)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) g[3 + j] = xs_g(R.ay, R.sy, uy[j], r.p.y[j]);
+    if (k.flags & XS_WAZ)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) g[6 + j] = xs_g(k.az, sz, uz[j], r.p.z[j]);
     if (owned) xs_psi_store(Q, R, k, r.p, ux, uy, uz);
 }
 
@@ -614,6 +628,8 @@ __device__ __forceinline__ void st_form(const StSrc &S, const XsPsiPtr &Q, const
     const float sxy = kdt * r.m[0] * r.b[3], sxz = kdt * r.m[1] * r.b[4], syz = kdt * r.m[2] * r.b[5];
     const bool sx = k.flags & XS_SX, sz = k.flags & XS_SZ;
     const float ex[3] = {exx, sxy, sxz}, ey[3] = {eyy, sxy, syz}, ez[3] = {ezz, sxz, syz};
+    // (the mixing is not branched here as in vt_form: in this kernel the branches cost more
+    // registers than they save instructions)
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
         o.d[q] = xs_g(k.ax, sx, ex[q], r.p.x[q]);

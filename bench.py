@@ -488,8 +488,12 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         from elastic_fm_vp_vs_rho_b200 import batchbench
-        batched = batchbench.run(argparse.Namespace(workload="uneven", n=48, steps=1, warmup=1,
-                                                    budget_gb=0.0, shots=32, nx=200, ny=200, nz=100))
+        try:
+            batched = batchbench.run(argparse.Namespace(workload="uneven", n=48, steps=1, warmup=1,
+                                                        budget_gb=0.0, shots=32, nx=200, ny=200,
+                                                        nz=100))
+        except Exception as e:  # the headline line is printed either way
+            batched = {"error": f"{type(e).__name__}: {e}"[:300]}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,

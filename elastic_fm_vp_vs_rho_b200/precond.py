@@ -509,8 +509,9 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
 def variant_experiment(variants, train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9),
                        iters=10, spec=None, log=None, illumination=True, policy="first2"):
     """Several networks trained on the SAME plain-L-BFGS runs (one data pass): each variant
-    is (target, epochs); on the unseen seeds every variant's learned run (one policy) is
-    compared with plain L-BFGS as in :func:`experiment`."""
+    is (target, epochs); on the unseen seeds every variant's learned run is compared with
+    plain L-BFGS as in :func:`experiment`, under each policy of ``policy`` (a name or a
+    comma list; with several, results are keyed "variant@policy")."""
     import time
     base = spec or ProblemSpec()
     raw = []
@@ -529,26 +530,28 @@ def variant_experiment(variants, train_seeds=tuple(range(100, 108)), test_seeds=
         nets[name] = net
         info[name] = dict(target=target, epochs=epochs, loss_first=losses[0], loss_last=losses[-1])
         del samples
-    kw = POLICIES[policy]
+    pols = [p for p in str(policy).split(",") if p]
+    runs = {(n if len(pols) == 1 else f"{n}@{p}"): (n, p) for n in nets for p in pols}
     tests = []
     for ts in test_seeds:
         prob = InversionProblem(dataclasses.replace(base, seed=ts), illumination)
         plain = invert(prob, iters, log=log)
         target_j = plain[-1]["misfit"]
         row = dict(seed=ts, target_misfit=target_j, solves_plain=plain[-1]["solves"], variants={})
-        for name, net in nets.items():
-            h = invert(prob, iters, net=net, log=log, **kw)
-            row["variants"][name] = dict(solves=solves_to_reach(h, target_j),
-                                         final_misfit=h[-1]["misfit"],
-                                         fallbacks=sum(x["used"] == "fallback" for x in h))
+        for key, (name, pol) in runs.items():
+            h = invert(prob, iters, net=nets[name], log=log, **POLICIES[pol])
+            row["variants"][key] = dict(solves=solves_to_reach(h, target_j),
+                                        final_misfit=h[-1]["misfit"],
+                                        fallbacks=sum(x["used"] == "fallback" for x in h))
         prob.batch.close()
         tests.append(row)
     summary = {}
-    for name in nets:
-        sv = [t["variants"][name]["solves"] for t in tests]
+    for key, (name, pol) in runs.items():
+        sv = [t["variants"][key]["solves"] for t in tests]
         plain_tot = sum(t["solves_plain"] for t in tests)
-        summary[name] = dict(info[name], solves=sv, solves_plain=[t["solves_plain"] for t in tests],
-                             total_ratio=(plain_tot / sum(sv)) if all(sv) else None)
+        summary[key] = dict(info[name], policy=pol, solves=sv,
+                            solves_plain=[t["solves_plain"] for t in tests],
+                            total_ratio=(plain_tot / sum(sv)) if all(sv) else None)
     return dict(spec=dataclasses.asdict(base), policy=policy, illumination=illumination,
                 train_seeds=list(train_seeds), test_seeds=list(test_seeds), iters=iters,
                 n_samples=len(raw), data_s=t_data, summary=summary, tests=tests)
@@ -588,7 +591,7 @@ if __name__ == "__main__":
                                                                nshots=a.shots, nrec=a.receivers,
                                                                dx=a.dx, lenpml=a.lenpml, fq=a.fq),
                                log=print, illumination=not a.no_illumination,
-                               policy=a.policies.split(",")[0])
+                               policy=a.policies)
         if a.out:
             with open(a.out, "w") as f:
                 f.write(json.dumps(r, indent=1))

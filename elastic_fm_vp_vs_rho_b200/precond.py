@@ -458,7 +458,8 @@ def solves_to_reach(hist, target):
 
 
 POLICIES = {"always": dict(learned_iters=None), "first2": dict(learned_iters=2),
-            "first4": dict(learned_iters=4)}
+            "first4": dict(learned_iters=4), "first6": dict(learned_iters=6),
+            "first8": dict(learned_iters=8)}
 
 
 def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=12, epochs=40,

@@ -768,13 +768,16 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
     bool xs_fits = true;
     for (const Inst &I : ctx->inst)
         xs_fits = xs_fits && 9 * I.ncell < ((int64_t)1 << 31) && psi_floats(I) < ((size_t)1 << 31);
+    // the streaming form indexes cells with 32-bit offsets (instances below ~238 M cells);
+    // larger batches run the per-cell + gather form
+    const int form = (ctx->opt_exact_form == 2 && !xs_fits) ? 0 : ctx->opt_exact_form;
     for (int i = 0; i < n; ++i) {
         Inst &I = ctx->inst[i];
         EFM_CK(cudaMemsetAsync(I.bv(0), 0, 9 * I.ncell * sizeof(float), s));
         EFM_CK(cudaMemsetAsync(I.apsi, 0, 2 * psi_floats(I) * sizeof(float), s));
         // the per-cell + gather forms' scratch (allocated on first use); cells outside the
         // update domain read zero from it
-        if (ctx->opt_exact_form != 2) {
+        if (form != 2) {
             if (I.exscr == nullptr &&
                 cudaMalloc(&I.exscr, 9 * (size_t)I.ncell * sizeof(float)) != cudaSuccess) {
                 cudaGetLastError();
@@ -886,8 +889,6 @@ int exact_gradient(efm_ctx *ctx, const float *res, float *grad, double *mtg, boo
                      return efm_launch_exact(0, t, n, 0, it, slot, s);
                  })))
                 return rc;
-            // the streaming form indexes cells with 32-bit offsets (instances below ~238 M cells)
-            const int form = (ctx->opt_exact_form == 2 && !xs_fits) ? 0 : ctx->opt_exact_form;
             const int kv = form == 1 ? 4 : 1, ks = form == 1 ? 5 : 2;
             if ((rc = timed_launch(ctx, EFM_K_ADJ_VELOCITY, s, [&] {
                      return form == 2 ? efm_launch_exact_stream(0, xs_rows, t, n, st_tiles, it, slot, s)

@@ -509,7 +509,7 @@ def experiment(train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9), iters=1
 
 
 def variant_experiment(variants, train_seeds=tuple(range(100, 108)), test_seeds=(7, 8, 9),
-                       iters=10, spec=None, log=None, illumination=True, policy="first2"):
+                       iters=10, spec=None, log=None, illumination=True, policy="first4"):
     """Several networks trained on the SAME plain-L-BFGS runs (one data pass): each variant
     is (target, epochs); on the unseen seeds every variant's learned run is compared with
     plain L-BFGS as in :func:`experiment`, under each policy of ``policy`` (a name or a
@@ -577,7 +577,7 @@ if __name__ == "__main__":
     ap.add_argument("--dx", type=float, default=10.0)
     ap.add_argument("--lenpml", type=int, default=8)
     ap.add_argument("--fq", type=float, default=12.0)
-    ap.add_argument("--policies", default="first2,always", help="comma list of " + ",".join(POLICIES))
+    ap.add_argument("--policies", default="first4,first2", help="comma list of " + ",".join(POLICIES))
     ap.add_argument("--out", default=None)
     ap.add_argument("--variants", default=None,
                     help="target:epochs,... -- several networks trained on one data pass")

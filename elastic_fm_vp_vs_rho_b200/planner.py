@@ -8,7 +8,9 @@ K + 1 stored steps for the exact gradient.  :func:`instance_bytes` restates thos
 allocations (efm_capi.cu: ensure_workspace, ensure_exact) plus the caller's buffers
 (gathers, residual, gradient); :func:`plan` packs instances into sub-batches (first fit,
 largest first) under ``budget`` bytes; :func:`choose_checkpoint_interval` picks the
-smallest checkpoint interval K whose exact-gradient workspace fits.
+smallest-memory checkpoint interval K whose exact-gradient workspace fits, and
+:func:`auto_checkpoint_interval` restates the library's automatic interval (the longest that
+fits).
 """
 from __future__ import annotations
 
@@ -61,6 +63,32 @@ def choose_checkpoint_interval(nx, ny, nz, lenpml, nt, budget, nrec=0):
         if K > 4 * math.isqrt(nt) + 4 and best_b is not None:
             break
     return best if best_b is not None and best_b <= budget else None
+
+
+def exact_workspace_bytes(nx, ny, nz, lenpml, nt, K):
+    """The exact adjoint's own workspace of one instance at checkpoint interval K (ensure_exact
+    in efm_capi.cu): nt/K - 1 checkpoints of the 9 fields and the memory variables, a segment
+    of K + 1 stored steps, the adjoint memory variables (two parities) and 6 harmonic-average
+    volumes."""
+    ncell, psi, _ = _geometry(nx, ny, nz, lenpml)
+    K = max(1, min(K, nt))
+    nck = max(1, (nt + K - 1) // K - 1)
+    return (nck * (9 * ncell + psi) + (K + 1) * 9 * ncell + 2 * psi + 6 * ncell) * 4
+
+
+def auto_checkpoint_interval(shapes, nt, budget):
+    """The interval EFM_OPT_CHECKPOINT_EVERY = 0 picks (checkpoint_interval in efm_capi.cu):
+    the longest K that splits nt into equal segments and whose workspace for every instance
+    fits in ``budget`` bytes (the library takes 60% of the free device memory), never below
+    ~sqrt(nt), the smallest-memory interval.  shapes: (nx, ny, nz, lenpml) per instance."""
+    kmin = max(1, math.isqrt(nt))
+    for nseg in range(1, nt + 1):
+        k = (nt + nseg - 1) // nseg
+        if k < kmin:
+            break
+        if sum(exact_workspace_bytes(*sh, nt, k) for sh in shapes) <= budget:
+            return k
+    return kmin
 
 
 def plan(sizes, budget):

@@ -1,4 +1,6 @@
 """Memory planner (CPU) and a planned, sub-batched gradient equal to one batch (GPU)."""
+import math
+
 import numpy as np
 import pytest
 
@@ -32,6 +34,28 @@ def test_checkpoint_interval_minimises_exact_workspace():
     for k in (1, 5, K // 2 or 1, 2 * K, nt):
         assert planner.instance_bytes(96, 96, 64, 10, nt, 0, "exact", k) >= b
     assert planner.choose_checkpoint_interval(96, 96, 64, 10, nt, 1000) is None
+
+
+def test_auto_checkpoint_interval_is_the_longest_equal_split_that_fits():
+    """The automatic interval: K = nt (no replay) when one segment fits, else the longest
+    K = ceil(nt / nseg) that fits, never below ~sqrt(nt); memory grows with K above that."""
+    from elastic_fm_vp_vs_rho_b200 import planner
+    sh = [(128, 128, 96, 10)]
+    nt = 300
+    one = planner.exact_workspace_bytes(*sh[0], nt, nt)
+    assert planner.auto_checkpoint_interval(sh, nt, one) == nt
+    assert planner.auto_checkpoint_interval(sh, nt, one - 1) == 150
+    K = planner.auto_checkpoint_interval(sh, nt, one // 4)
+    assert planner.exact_workspace_bytes(*sh[0], nt, K) <= one // 4
+    assert K >= math.isqrt(nt) and K == -(-nt // -(-nt // K))  # an equal split of nt
+    # a longer equal split would not fit
+    nseg = -(-nt // K)
+    assert planner.exact_workspace_bytes(*sh[0], nt, -(-nt // (nseg - 1))) > one // 4
+    assert planner.auto_checkpoint_interval(sh, nt, 0) == math.isqrt(nt)
+    # two instances share the budget
+    assert planner.auto_checkpoint_interval(sh * 2, nt, one) < nt
+    # the bench workload on a B200: 2000 steps of 256 x 256 x 128 in 60% of ~178 GB
+    assert planner.auto_checkpoint_interval([(256, 256, 128, 10)], 2000, int(0.6 * 178e9)) == 334
 
 
 def test_uneven_instances_are_seeded_and_in_range():
